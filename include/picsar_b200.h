@@ -1,0 +1,303 @@
+/*
+ * picsar_b200.h -- C ABI of libpicsar_b200.so, the B200 (sm_100a) kernels
+ * behind PICSAR's per-step particle loop.
+ *
+ * Conventions
+ *  - Every entry point returns int: 0 on success, otherwise a PXRB_E* code.
+ *  - Array arguments are DEVICE pointers unless stated otherwise; bounds
+ *    arrays of the Yee routines (int64_t[3]) are HOST pointers.
+ *  - Grids follow PICSAR's Fortran layout: float64, column-major (x fastest),
+ *    lower bound -guard and upper bound n+guard per axis; the pointer
+ *    addresses element (-gx,-gy,-gz).
+ *  - Fortran INTEGER(idp) -> int64_t, REAL(num) -> double,
+ *    LOGICAL(lp) -> int64_t (0 = .FALSE.).
+ *  - Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
+ *    stream); no entry point synchronises the device.
+ *  - Module variables the Fortran routines read implicitly (`dt`,
+ *    `particle_pusher`, `clight`) are explicit trailing arguments.
+ *  - Gather and deposition ACCUMULATE into their outputs, as the reference
+ *    does; the caller zeroes them.
+ *
+ * Reference citations are paths inside the PICSAR source tree.
+ */
+#ifndef PICSAR_B200_H
+#define PICSAR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PXRB_OK 0
+#define PXRB_EINVAL 1
+#define PXRB_EUNSUPPORTED 2
+#define PXRB_ELAUNCH 3
+#define PXRB_ESCRATCH 4
+#define PXRB_ERANGE 5
+
+/* ------------------------------------------------------------------------
+ * Plain FP64 path (PICSAR arrays, one thread per particle, FP64 atomics)
+ * ---------------------------------------------------------------------- */
+
+/* Replaces field_gathering_plus_particle_pusher_{1_1_1,2_2_2,3_3_3}
+ * (src/particle_pushers/particle_pusher_manager_3d.F90:1287, :1522, :1820):
+ * energy-conserving gather (+=) into ex..bz, then Boris + pxr_set_gamma
+ * (particle_pusher = 0) or Vay (1), then pxr_pushxyz, all with `dt`.
+ * Only l_lower_order_in_v = .TRUE. exists in the reference fused kernels.
+ * `order` selects 1, 2 or 3; the three _n_n_n symbols below fix it. */
+int pxrb_field_gathering_plus_particle_pusher(
+    int64_t order, int64_t np, double* xp, double* yp, double* zp, double* uxp, double* uyp,
+    double* uzp, double* gaminv, double* ex, double* ey, double* ez, double* bx, double* by,
+    double* bz, double xmin, double ymin, double zmin, double dx, double dy, double dz,
+    double dtt, int64_t nx, int64_t ny, int64_t nz, int64_t nxguard, int64_t nyguard,
+    int64_t nzguard, const double* exg, const double* eyg, const double* ezg,
+    const double* bxg, const double* byg, const double* bzg, double q, double m,
+    int64_t lvect, int64_t l_lower_order_in_v, double dt, int64_t particle_pusher,
+    double clight, void* stream);
+#define PXRB_FGP_DECL(O)                                                                  \
+  int pxrb_field_gathering_plus_particle_pusher_##O##_##O##_##O(                          \
+      int64_t np, double* xp, double* yp, double* zp, double* uxp, double* uyp,           \
+      double* uzp, double* gaminv, double* ex, double* ey, double* ez, double* bx,        \
+      double* by, double* bz, double xmin, double ymin, double zmin, double dx, double dy, \
+      double dz, double dtt, int64_t nx, int64_t ny, int64_t nz, int64_t nxguard,         \
+      int64_t nyguard, int64_t nzguard, const double* exg, const double* eyg,             \
+      const double* ezg, const double* bxg, const double* byg, const double* bzg,         \
+      double q, double m, int64_t lvect, int64_t l_lower_order_in_v, double dt,           \
+      int64_t particle_pusher, double clight, void* stream);
+/* particle_pusher_manager_3d.F90:1287 */
+PXRB_FGP_DECL(1)
+/* particle_pusher_manager_3d.F90:1522 */
+PXRB_FGP_DECL(2)
+/* particle_pusher_manager_3d.F90:1820 */
+PXRB_FGP_DECL(3)
+#undef PXRB_FGP_DECL
+
+/* Replaces geteb3d_energy_conserving
+ * (src/field_gathering/field_gathering_manager_3d.F90:295-323): separate
+ * gather (+=), both l_lower_order_in_v branches, l_nodal as the nodal-grid
+ * module flag.  nox = noy = noz in 1..3; ll4symtry must be 0. */
+int pxrb_geteb3d_energy_conserving(
+    int64_t np, const double* xp, const double* yp, const double* zp, double* ex, double* ey,
+    double* ez, double* bx, double* by, double* bz, double xmin, double ymin, double zmin,
+    double dx, double dy, double dz, int64_t nx, int64_t ny, int64_t nz, int64_t nxguard,
+    int64_t nyguard, int64_t nzguard, int64_t nox, int64_t noy, int64_t noz,
+    const double* exg, const double* eyg, const double* ezg, const double* bxg,
+    const double* byg, const double* bzg, int64_t ll4symtry, int64_t l_lower_order_in_v,
+    int64_t lvect, int64_t field_gathe_algo, int64_t l_nodal, void* stream);
+
+/* Replaces pxr_boris_push_u_3d (src/particle_pushers/boris_pusher/boris_3d.F90:51). */
+int pxrb_boris_push_u_3d(int64_t np, double* uxp, double* uyp, double* uzp, double* gaminv,
+                         const double* ex, const double* ey, const double* ez,
+                         const double* bx, const double* by, const double* bz, double q,
+                         double m, double dt, double clight, void* stream);
+
+/* Replaces pxr_ebcancelpush3d (src/particle_pushers/vay_pusher/vay_3d.F90:56),
+ * which = 0 (full push), 1 (first half), 2 (second half). */
+int pxrb_ebcancelpush3d(int64_t np, double* uxp, double* uyp, double* uzp, double* gi,
+                        const double* ex, const double* ey, const double* ez,
+                        const double* bx, const double* by, const double* bz, double q,
+                        double m, double dt, int64_t which, double clight, void* stream);
+
+/* Replaces pxr_set_gamma (boris_3d.F90:1059). */
+int pxrb_set_gamma(int64_t np, const double* uxp, const double* uyp, const double* uzp,
+                   double* gaminv, double clight, void* stream);
+
+/* Replaces pxr_pushxyz (boris_3d.F90:849). */
+int pxrb_pushxyz(int64_t np, double* xp, double* yp, double* zp, const double* uxp,
+                 const double* uyp, const double* uzp, const double* gaminv, double dt,
+                 void* stream);
+
+/* Replaces depose_jxjyjz (current_depo_algo = 0: specialised Esirkepov
+ * depose_jxjyjz_esirkepov_{1,2,3}) and depose_jxjyjz_esirkepov
+ * (current_depo_algo = 1: pxr_depose_jxjyjz_esirkepov_n with its
+ * xold + dt*v reconstruction) (src/particle_deposition/current_deposition/
+ * current_deposition_manager_3d.F90:47, :75; esirkepov/esirkepov_3d.F90:82,
+ * :1734, :3263, :3480).  Accumulates; nox = noy = noz in 1..3.
+ * err_flag (device int) is set to 1 if a particle moved more than one cell
+ * per axis in one step (impossible under the CFL limit). */
+int pxrb_depose_jxjyjz(double* jx, double* jy, double* jz, int64_t np, const double* xp,
+                       const double* yp, const double* zp, const double* uxp,
+                       const double* uyp, const double* uzp, const double* gaminv,
+                       const double* w, double q, double xmin, double ymin, double zmin,
+                       double dt, double dx, double dy, double dz, int64_t nx, int64_t ny,
+                       int64_t nz, int64_t nxguard, int64_t nyguard, int64_t nzguard,
+                       int64_t nox, int64_t noy, int64_t noz, int64_t current_depo_algo,
+                       int* err_flag, void* stream);
+
+/* Replaces depose_rho_scalar_{1,2,3}_{1,2,3}_{1,2,3}
+ * (src/particle_deposition/charge_deposition/charge_deposition_3d.F90:77,
+ * :174, :324).  Accumulates node-centred rho. */
+int pxrb_depose_rho(int64_t order, double* rho, int64_t np, const double* xp,
+                    const double* yp, const double* zp, const double* w, double q,
+                    double xmin, double ymin, double zmin, double dx, double dy, double dz,
+                    int64_t nx, int64_t ny, int64_t nz, int64_t nxguard, int64_t nyguard,
+                    int64_t nzguard, void* stream);
+
+/* Replaces pxrpush_em3d_evec (src/field_solvers/Maxwell/yee_solver/yee.F90:637).
+ * x/y/z lo/hi: loop ranges of Ex/Ey/Ez; <a>lo/<a>hi: array bounds (HOST). */
+int pxrb_push_em3d_evec(const int64_t* xlo, const int64_t* xhi, const int64_t* ylo,
+                        const int64_t* yhi, const int64_t* zlo, const int64_t* zhi,
+                        double* ex, const int64_t* exlo, const int64_t* exhi, double* ey,
+                        const int64_t* eylo, const int64_t* eyhi, double* ez,
+                        const int64_t* ezlo, const int64_t* ezhi, const double* bx,
+                        const int64_t* bxlo, const int64_t* bxhi, const double* by,
+                        const int64_t* bylo, const int64_t* byhi, const double* bz,
+                        const int64_t* bzlo, const int64_t* bzhi, const double* jx,
+                        const int64_t* jxlo, const int64_t* jxhi, const double* jy,
+                        const int64_t* jylo, const int64_t* jyhi, const double* jz,
+                        const int64_t* jzlo, const int64_t* jzhi, double mudt, double dtsdx,
+                        double dtsdy, double dtsdz, void* stream);
+
+/* Replaces pxrpush_em3d_bvec (yee.F90:1258). */
+int pxrb_push_em3d_bvec(const int64_t* xlo, const int64_t* xhi, const int64_t* ylo,
+                        const int64_t* yhi, const int64_t* zlo, const int64_t* zhi,
+                        const double* ex, const int64_t* exlo, const int64_t* exhi,
+                        const double* ey, const int64_t* eylo, const int64_t* eyhi,
+                        const double* ez, const int64_t* ezlo, const int64_t* ezhi,
+                        double* bx, const int64_t* bxlo, const int64_t* bxhi, double* by,
+                        const int64_t* bylo, const int64_t* byhi, double* bz,
+                        const int64_t* bzlo, const int64_t* bzhi, double dtsdx, double dtsdy,
+                        double dtsdz, void* stream);
+
+/* Replaces field_bc -> exchange_mpi_3d_grid_array_with_guards for a single
+ * periodic domain (src/boundary_conditions/field_boundaries.F90:81-269), for
+ * one to three grids of the same shape (f2/f3 may be NULL).  Needs n > g. */
+int pxrb_field_bc_periodic(double* f1, double* f2, double* f3, int64_t nx, int64_t ny,
+                           int64_t nz, int64_t nxg, int64_t nyg, int64_t nzg, void* stream);
+
+/* Replaces summation_bcs (field_boundaries.F90:403-503) for a single periodic
+ * domain: fold the guards into the interior, then field_bc. */
+int pxrb_summation_bcs_periodic(double* f1, double* f2, double* f3, int64_t nx, int64_t ny,
+                                int64_t nz, int64_t nxg, int64_t nyg, int64_t nzg,
+                                void* stream);
+
+/* Replaces the periodic branch (pbound = 0) of the particle boundary
+ * conditions (src/boundary_conditions/particle_boundaries.F90:1109-1300). */
+int pxrb_particle_bcs_periodic(int64_t np, double* xp, double* yp, double* zp, double xmin,
+                               double ymin, double zmin, double xmax, double ymax,
+                               double zmax, void* stream);
+
+
+/* ------------------------------------------------------------------------
+ * Tiled engine (B200-native layout): FP32 mixed precision or FP64.
+ *
+ * One pxrb_tiled_job describes one periodic simulation.  Fields E, B are
+ * stored with `g` periodic guard cells per side in arrays of extent
+ * (pitch_x, ny+2g, nz+2g), x fastest, element (i,j,k) at
+ * (i+g) + pitch_x*((j+g) + (ny+2g)*(k+g)); the current J is FP64 without
+ * guards (nx*ny*nz, periodic indexing).  Particles are SoA sorted by cell
+ * tile: a packed cell index (x | y<<11 | z<<22; nx, ny <= 2048, nz <= 1024)
+ * plus an in-cell offset in [0,1) per axis, momenta u = gamma*beta and the
+ * weight, all in the engine precision.  `prec` selects float (0) or double
+ * (1) for fields, offsets, momenta and weights.  `tile_off[t]..tile_off[t+1]`
+ * is the particle range of tile t (tiles x fastest).
+ * ---------------------------------------------------------------------- */
+typedef struct pxrb_tiled_job {
+  int32_t nx, ny, nz;        /* cells per axis (periodic) */
+  int32_t tx, ty, tz;        /* tile size in cells */
+  int32_t ntx, nty, ntz;     /* tiles per axis = ceil(n / t) */
+  int32_t g;                 /* guard cells of the E/B arrays (>= 3) */
+  int32_t pitch_x;           /* allocated x extent of the E/B arrays (>= nx+2g) */
+  int32_t order;             /* shape order 1..3 */
+  int32_t pusher;            /* 0 Boris (+ set_gamma), 1 Vay */
+  int32_t drift;             /* window margin (cells) around each tile */
+  int32_t prec;              /* 0 float, 1 double */
+  int32_t pad0;
+  int64_t np;                /* particles */
+  double dx, dy, dz, dt, q, m, clight, mu0, eps0, xmin, ymin, zmin;
+  void *ex, *ey, *ez, *bx, *by, *bz;        /* guarded, engine precision */
+  double *jx, *jy, *jz;                     /* nx*ny*nz */
+  uint32_t* cell;                           /* packed cell index */
+  void *ox, *oy, *oz, *ux, *uy, *uz, *w;    /* engine precision */
+  uint32_t* cell_b;                         /* sort output buffers */
+  void *ox_b, *oy_b, *oz_b, *ux_b, *uy_b, *uz_b, *w_b;
+  int32_t *pid, *pid_b;                     /* optional particle ids (NULL: none),
+                                               permuted by the sort only */
+  int32_t* tile_off;                        /* ntiles + 1 */
+  int32_t* tile_cnt;                        /* ntiles + 1 (sort scratch) */
+  double* ke_tile;                          /* ntiles: kinetic energy per tile */
+  int32_t* counters;                        /* [0] particles on the slow path,
+                                               [1] error flag */
+} pxrb_tiled_job;
+
+/* Fused per-step particle kernel of the tiled engine: energy-conserving
+ * gather (l_lower_order_in_v), Boris or Vay push, position push, periodic
+ * wrap, and Esirkepov deposition from the exact old position into J (+=).
+ * Restates, fused, field_gathering_plus_particle_pusher_{n}_{n}_{n}
+ * (particle_pusher_manager_3d.F90:1287-2193), particle_bcs (periodic,
+ * particle_boundaries.F90:1109-1300) and depose_jxjyjz_esirkepov_{n}_{n}_{n}
+ * (esirkepov_3d.F90:82, :1734, :3263).  Persistent CTAs pull (job, tile)
+ * items; the tile's E/B window and J accumulator live in shared memory;
+ * particles that left the window since the last sort take a global-memory
+ * path.  jobs_dev: DEVICE descriptors (all of this `order` and `prec`);
+ * work: DEVICE int32 pairs (job, tile), nwork of them (nwork_dev, if not
+ * NULL, a DEVICE count <= nwork read at run time); ctr: DEVICE int32 reset by
+ * the call; threads: CTA size, multiple of 32, <= 256; smem: dynamic shared
+ * memory bytes, >= pxrb_tiled_smem_bytes() of the largest tile window. */
+int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int32_t prec,
+                             const int32_t* work, int32_t nwork, const int32_t* nwork_dev,
+                             int32_t* ctr, int32_t threads, int32_t ctas, int64_t smem,
+                             void* stream);
+
+/* sizeof(pxrb_tiled_job), for bindings that mirror the struct. */
+int64_t pxrb_tiled_job_size(void);
+
+/* Dynamic shared memory the particle kernel needs for a tile shape, order,
+ * window margin and precision (host function, no GPU work). */
+int64_t pxrb_tiled_smem_bytes(int32_t order, int32_t prec, int32_t tx, int32_t ty,
+                              int32_t tz, int32_t drift);
+
+/* Yee steps on the engine layout, every job in one launch (yee.F90:1258-1347
+ * and :637-740; periodic guard images written by the same kernel).
+ * push_b: B -= frac*dt*curl E.  push_e: E += c^2 dt curl B - c^2 mu0 dt J,
+ * then J = 0 when zero_j != 0.  cell_off_dev: DEVICE int64[njobs+1], start of
+ * each job in a flat cell index whose job segments are padded to multiples of
+ * 256; total_cells = cell_off[njobs] (host value). */
+int pxrb_tiled_push_b(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
+                      const int64_t* cell_off_dev, int64_t total_cells, double frac,
+                      void* stream);
+int pxrb_tiled_push_e(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
+                      const int64_t* cell_off_dev, int64_t total_cells, int32_t zero_j,
+                      void* stream);
+
+/* Counting sort of one job's particles by cell tile: the B200 form of
+ * pxr_particle_sorting (src/housekeeping/sorting.F90:67-361) with the tile of
+ * the particle's cell as key; order inside a tile is unspecified.  Rebuilds
+ * tile_off and swaps, in the DEVICE descriptor, the particle arrays with
+ * their *_b buffers.  job_host: host copy (sizes, tile_cnt, tile_off). */
+int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, void* stream);
+
+/* Conversions between PICSAR's particle arrays (absolute FP64 positions,
+ * u, weight; DEVICE) and the engine SoA of one job (unsorted after a load:
+ * call pxrb_tiled_sort), and between PICSAR's guarded FP64 Fortran grids
+ * (nguard guards) and the engine: which 0..5 = ex..bz, 6..8 = jx..jz.
+ * job_host must hold the current particle pointers (after sorts, read the
+ * device descriptor back first). */
+int pxrb_tiled_load_particles(const pxrb_tiled_job* job_host, const double* x,
+                              const double* y, const double* z, const double* ux,
+                              const double* uy, const double* uz, const double* w,
+                              void* stream);
+int pxrb_tiled_store_particles(const pxrb_tiled_job* job_host, double* x, double* y,
+                               double* z, double* ux, double* uy, double* uz,
+                               double* gaminv, double* w, void* stream);
+int pxrb_tiled_field_import(const pxrb_tiled_job* job_host, int32_t which, const double* src,
+                            int64_t nguard_src, void* stream);
+int pxrb_tiled_field_export(const pxrb_tiled_job* job_host, int32_t which, double* dst,
+                            int64_t nguard_dst, void* stream);
+
+/* FP64 diagnostics of one job (diags.F90:847-1358): out[0] kinetic energy
+ * sum (gamma-1) w m c^2 (from ke_tile, written by the particle kernel),
+ * out[1..3] E energies (sum 0.5 F^2 dV * eps0), out[4..6] B energies
+ * (/ mu0), out[7] || div E * eps0 - rho ||_2 and out[8] || rho ||_2 over the
+ * periodic domain, with rho (DEVICE FP64 nx*ny*nz) zeroed and deposited here.
+ * scratch: DEVICE double[scratch_len], scratch_len >= pxrb_tiled_diag_scratch();
+ * out: DEVICE double[9]. */
+int64_t pxrb_tiled_diag_scratch(const pxrb_tiled_job* job_host);
+int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* scratch,
+                           int64_t scratch_len, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PICSAR_B200_H */
