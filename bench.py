@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of the PIC step (particle-steps/s) on one B200 per rank.
+
+Workload ("large"): periodic homogeneous thermal electron plasma, 256^3
+cells, 8 particles per cell (134,217,728 electrons), u ~ N(0, 0.01^2) per
+component, order-3 shapes, Boris pusher, 8^3 cell tiles, re-sort every 20
+steps, 2nd-order Yee at 0.95 CFL, normalized units (c = mu0 = eps0 = 1,
+dx = 1), FP32 mixed precision (FP64 J flush and energy sums).  Synthetic
+seeded input stands in for the reference's decks.  A step is one full PIC
+step: fused gather/push/deposit kernel, B/E/B Yee pushes, and the periodic
+counting sort every 20 steps.
+
+Arms:
+  (default)          this framework; also reports the plain FP64 GPU path,
+                     the end-to-end host-buffer run, the CPU oracle
+                     baseline, a roofline of the fused particle kernel and
+                     the SM clocks sampled during the timed region.
+  --impl reference   the reference algorithm on the host CPU cores: the
+                     C++ restatement of PICSAR's Fortran routines (the
+                     Fortran itself cannot be compiled here), OpenMP over
+                     the reference's tile loops, on a bounded sample.
+
+Multi-GPU: independent replicas, one per rank (no data-path collective);
+value = particle-steps of all ranks / max over ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "large": dict(n=(256, 256, 256), ppc=8, order=3, tile=(8, 8, 8), sort_interval=20,
+                  sigma=0.01, pusher=0,
+                  desc="256^3 cells, 8 ppc (134,217,728 electrons), order 3, tiles 8^3, "
+                       "re-sort every 20 steps, Boris, u_th 0.01, periodic"),
+    "medium": dict(n=(128, 128, 64), ppc=8, order=3, tile=(8, 8, 8), sort_interval=20,
+                   sigma=0.01, pusher=0,
+                   desc="128x128x64 cells, 8 ppc (8,388,608 electrons), order 3, tiles 8^3, "
+                        "re-sort every 20 steps, Boris, u_th 0.01, periodic (profiling size)"),
+    "plain-small": dict(n=(32, 32, 32), ppc=8, order=1, tile=(8, 8, 8), sort_interval=20,
+                        sigma=0.01, pusher=0,
+                        desc="32^3 cells, 8 ppc (262,144 electrons), order 1, Boris, u_th 0.01"),
+}
+BYTES_PER_PARTICLE = {0: (32 + 28), 1: (60 + 52)}        # particle kernel, per particle
+GRID_BYTES_PER_CELL = {0: (24 + 48), 1: (48 + 48)}        # E,B read + J FP64 read-modify-write
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    def __init__(self, dev_index):
+        import torch
+        self.proc = None
+        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_rank{dev_index}.csv")
+        try:
+            bus = torch.cuda.get_device_properties(dev_index).pci_bus_id
+        except Exception:
+            bus = str(dev_index)
+        self.bus = bus
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.out), exist_ok=True)
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.out, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.bus, f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.out) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def _dist():
+    import torch
+    import torch.distributed as dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1 and not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def _max_over_ranks(x, ws):
+    import torch
+    import torch.distributed as dist
+    if ws == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+# ---------------------------------------------------------------------------
+def cpu_oracle_rate(wl, steps, warmup, threads=None):
+    """Oracle (C++ restatement of the reference routines, OpenMP over tiles)
+    on a 32^3-cell sample of the workload: returns particle-steps/s."""
+    from oracle import oracle as O
+    from picsar_b200.init import thermal_plasma
+    n = (32, 32, 32)
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    st = thermal_plasma(n, wl["ppc"], wl["sigma"], seed=11).numpy()
+    sim = O.OracleSim(n, 3, order=wl["order"], pusher=wl["pusher"], tiles=(4, 4, 4),
+                      sorting_period=wl["sort_interval"])
+    sim.add_particles(st["x"], st["y"], st["z"], st["ux"], st["uy"], st["uz"], st["w"])
+    np_ = len(st["x"])
+    sim.step(warmup)
+    t0 = time.perf_counter()
+    sim.step(steps)
+    el = time.perf_counter() - t0
+    return np_ * steps / el, el, np_, O.num_threads()
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = WORKLOADS[args.workload]
+    threads = os.cpu_count()
+    rate, el, np_, nth = cpu_oracle_rate(wl, args.steps, args.warmup, threads)
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": rate,
+        "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "sample": f"32^3 cells, {np_} particles per step"},
+        "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": nth,
+                         "kind": "port",
+                         "sample": f"{args.steps} PIC steps of a 32^3-cell, {np_}-particle "
+                                   f"sample of the workload, tiles 4^3, OpenMP"},
+        "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "PICSAR's Fortran cannot be compiled in this image (no Fortran compiler); "
+                "the reference arm runs the line-by-line C++ restatement of its routines",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    from picsar_b200.init import thermal_plasma
+    from picsar_b200.tiled import TiledConfig, TiledSim
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    wl = WORKLOADS[args.workload]
+    prec = 0 if args.precision == "fp32" else 1
+    cfg = TiledConfig(tile=wl["tile"], sort_interval=wl["sort_interval"], drift=1,
+                      threads=args.threads, ctas_per_sm=args.ctas_per_sm)
+    st = thermal_plasma(wl["n"], wl["ppc"], wl["sigma"], seed=1234 + rank, device="cuda")
+    N = st.np
+    sim = TiledSim(wl["n"], order=wl["order"], pusher=wl["pusher"], precision=args.precision,
+                   config=cfg)
+    sim.load_state(st)
+    for _ in range(args.warmup):
+        sim.step(1)
+    torch.cuda.synchronize()
+    e0 = sim.diagnostics(gauss=False)
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    launches0 = sim.launches
+    _barrier(ws)
+    clocks.start()
+    t_start.record(stream)
+    for s in range(args.steps):
+        sim.step(1, events=ev[s])
+    t_end.record(stream)
+    _barrier(ws)
+    clk = clocks.stop()
+    ms_total = t_start.elapsed_time(t_end)
+    ms_total = _max_over_ranks(ms_total, ws)
+    kern_ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    launches = sim.launches - launches0
+    e1 = sim.diagnostics(gauss=False)
+    slow = sim.slow_path_count()
+    value = N * ws * args.steps / (ms_total * 1e-3)
+
+    # roofline of the fused particle kernel
+    peak, peak_kind = _peaks()
+    ncell = wl["n"][0] * wl["n"][1] * wl["n"][2]
+    alg_bytes = BYTES_PER_PARTICLE[prec] * N + GRID_BYTES_PER_CELL[prec] * ncell
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "particle_kernel_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        key = f"{args.workload}_{args.precision}"
+        if key in tj:
+            traffic = tj[key]["dram_bytes_per_launch"]
+
+    # end-to-end through the public API with host buffers
+    e2e = None
+    if not args.skip_e2e:
+        e2e = run_e2e(sim, st, wl, args, ws)
+    del st
+
+    # plain FP64 GPU path on the same workload (the comparison baseline)
+    fp64 = None
+    if not args.skip_fp64:
+        del sim
+        torch.cuda.empty_cache()
+        fp64 = run_plain_fp64(wl, args, ws, rank)
+
+    cpu = None
+    if rank == 0 and not args.skip_cpu:
+        rate, el, np_, nth = cpu_oracle_rate(wl, args.cpu_steps, 1, os.cpu_count())
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": nth, "kind": "port",
+               "sample": f"{args.cpu_steps} PIC steps of a 32^3-cell, {np_}-particle sample "
+                         f"of the workload (oracle, OpenMP over 4^3 tiles), {el:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if prec == 0 else "f64", "data": "synthetic",
+            "config": {"workload": wl["desc"],
+                       "precision": "FP32 mixed (FP64 J flush and energy sums)" if prec == 0
+                       else "FP64", "particles_per_gpu": N, "cells": ncell,
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (particle SoA "
+                             f"{N * 32 / 1e9:.1f} GB per GPU), no flush",
+                       "tuning": {"tile": list(wl["tile"]), "drift": cfg.drift,
+                                  "threads": cfg.threads, "ctas_per_sm": cfg.ctas_per_sm,
+                                  "sort_interval": cfg.sort_interval}},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": f"k_tiled_step<{'float' if prec == 0 else 'double'},"
+                                   f"{wl['order']}>",
+                         "kernel_ms": kern_ms, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "fp64_plain": fp64,
+            "energy": {"start": e0["total"], "end": e1["total"],
+                       "rel_change": (e1["total"] - e0["total"]) / e0["total"]},
+            "slow_path_particle_steps": slow,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(sim, st, wl, args, ws):
+    """Same job through the public API from pinned host buffers: upload the
+    PICSAR particle arrays, run the steps reading the energies back every
+    step, download the final particle arrays."""
+    import torch
+    N = st.np
+    host = {c: getattr(st, c).to("cpu").pin_memory() for c in ("x", "y", "z", "ux", "uy", "uz", "w")}
+    dev = {c: torch.empty(N, dtype=torch.float64, device="cuda") for c in host}
+    out_host = {c: torch.empty(N, dtype=torch.float64).pin_memory()
+                for c in ("x", "y", "z", "ux", "uy", "uz", "gaminv", "w")}
+    diag_host = torch.empty((args.steps, 9), dtype=torch.float64).pin_memory()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(ws)
+    w0 = time.perf_counter()
+    a.record(stream)
+    for c in host:
+        dev[c].copy_(host[c], non_blocking=True)
+    sim.load_particles(dev["x"], dev["y"], dev["z"], dev["ux"], dev["uy"], dev["uz"], dev["w"])
+    for s in range(args.steps):
+        sim.step(1)
+        d = sim.diagnostics(gauss=False, to_host=False)
+        diag_host[s].copy_(d, non_blocking=True)
+    out = sim.particles()
+    for c in out_host:
+        out_host[c].copy_(out[c], non_blocking=True)
+    b.record(stream)
+    _barrier(ws)
+    wall = time.perf_counter() - w0
+    ms = _max_over_ranks(a.elapsed_time(b), ws)
+    h2d = 7 * 8 * N
+    d2h = 8 * 8 * N + args.steps * 9 * 8
+    return {"value": N * ws * args.steps / (ms * 1e-3), "unit": "particle-steps/s",
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "ms": ms, "wall_s": wall,
+            "what": "job: PICSAR arrays uploaded from pinned host memory, converted and "
+                    "sorted, all steps with the energies read back every step, final "
+                    "particle arrays downloaded"}
+
+
+def run_plain_fp64(wl, args, ws, rank):
+    """The plain FP64 GPU path (PICSAR arrays, FP64 atomics) on the workload."""
+    import torch
+    from picsar_b200.init import thermal_plasma
+    from picsar_b200.picsar import PicsarModule
+    st = thermal_plasma(wl["n"], wl["ppc"], wl["sigma"], seed=1234 + rank, device="cuda")
+    m = PicsarModule(*wl["n"], nguards=3, nox=wl["order"], particle_pusher=wl["pusher"])
+    m.add_species("electron", -1.0, 1.0, st.x, st.y, st.z, st.ux, st.uy, st.uz, st.w)
+    N = st.np
+    del st
+    m.step(1)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(ws)
+    a.record(stream)
+    m.step(args.fp64_steps)
+    b.record(stream)
+    _barrier(ws)
+    ms = _max_over_ranks(a.elapsed_time(b), ws)
+    del m
+    torch.cuda.empty_cache()
+    return {"value": N * ws * args.fp64_steps / (ms * 1e-3), "unit": "particle-steps/s",
+            "steps": args.fp64_steps, "ms_per_step": ms / args.fp64_steps,
+            "what": "plain FP64 GPU path: PICSAR guarded FP64 arrays, one thread per "
+                    "particle, global FP64 atomics, separate bc kernels"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="large", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--ctas-per-sm", type=int, default=2)
+    ap.add_argument("--fp64-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -290,7 +290,8 @@ int pxrb_tiled_field_export(const pxrb_tiled_job* job_host, int32_t which, doubl
  * sum (gamma-1) w m c^2 (from ke_tile, written by the particle kernel),
  * out[1..3] E energies (sum 0.5 F^2 dV * eps0), out[4..6] B energies
  * (/ mu0), out[7] || div E * eps0 - rho ||_2 and out[8] || rho ||_2 over the
- * periodic domain, with rho (DEVICE FP64 nx*ny*nz) zeroed and deposited here.
+ * periodic domain, with rho (DEVICE FP64 nx*ny*nz) zeroed and deposited here;
+ * rho = NULL computes the energies only (out[7], out[8] = 0).
  * scratch: DEVICE double[scratch_len], scratch_len >= pxrb_tiled_diag_scratch();
  * out: DEVICE double[9]. */
 int64_t pxrb_tiled_diag_scratch(const pxrb_tiled_job* job_host);

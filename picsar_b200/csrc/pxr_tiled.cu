@@ -781,13 +781,15 @@ __global__ void __launch_bounds__(RED_TPB) k_field_sums(Job J, const double* rho
       double v = (double)F[q][c];
       acc[q] += v * v * 0.5;
     }
-    double dive = ((double)F[0][c] - (double)F[0][c - 1]) / J.dx +
-                  ((double)F[1][c] - (double)F[1][c - sy]) / J.dy +
-                  ((double)F[2][c] - (double)F[2][c - sz]) / J.dz;
-    double r = rho[t];
-    double d = dive * J.eps0 - r;
-    acc[6] += d * d;
-    acc[7] += r * r;
+    if (rho) {
+      double dive = ((double)F[0][c] - (double)F[0][c - 1]) / J.dx +
+                    ((double)F[1][c] - (double)F[1][c - sy]) / J.dy +
+                    ((double)F[2][c] - (double)F[2][c - sz]) / J.dz;
+      double r = rho[t];
+      double d = dive * J.eps0 - r;
+      acc[6] += d * d;
+      acc[7] += r * r;
+    }
   }
   __shared__ double red[8][RED_TPB / 32];
   for (int q = 0; q < 8; ++q) {
@@ -1005,14 +1007,14 @@ int64_t pxrb_tiled_diag_scratch(const pxrb_tiled_job* job_host) {
 
 int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* scratch,
                            int64_t scratch_len, double* out, void* stream) {
-  if (!job_host || !rho || !scratch || !out) return PXRB_EINVAL;
+  if (!job_host || !scratch || !out) return PXRB_EINVAL;
   const Job& J = *job_host;
   const int nb = diag_blocks(J);
   if (scratch_len < 8 * (int64_t)nb) return PXRB_ESCRATCH;
   cudaStream_t s = (cudaStream_t)stream;
-  if (cudaMemsetAsync(rho, 0, sizeof(double) * (size_t)J.nx * J.ny * J.nz, s) != cudaSuccess)
+  if (rho && cudaMemsetAsync(rho, 0, sizeof(double) * (size_t)J.nx * J.ny * J.nz, s) != cudaSuccess)
     return PXRB_ELAUNCH;
-  if (J.np > 0) {
+  if (rho && J.np > 0) {
     const int pb = gs_blocks(J.np, 256);
 #define PXRB_RHO(R_)                                                   \
     if (J.order == 1) k_rho_t<R_, 1><<<pb, 256, 0, s>>>(J, rho);       \

@@ -141,6 +141,7 @@ class TiledSim:
         self.track_ids = track_ids
         self.np = 0
         self.it = 0
+        self.launches = 0          # kernels of this library launched so far
         self.smem = smem_bytes(self.order, self.prec, tile, cfg.drift)
         props = torch.cuda.get_device_properties(self.device)
         self.num_sms = props.multi_processor_count
@@ -237,35 +238,43 @@ class TiledSim:
 
     # -------------------------------------------------------------- stepping
     def sort(self):
-        self._pull_job_sizes_only()
+        # sizes, tile_cnt and tile_off of the host descriptor never change;
+        # the particle pointers it holds may be stale (the device swaps them)
         _lib.call("pxrb_tiled_sort", self._jp(), self.job_dev.data_ptr(), _stream())
-
-    def _pull_job_sizes_only(self):
-        pass  # sizes, tile_cnt and tile_off never change on the device
+        self.launches += 4 if self.np > 0 else 1
 
     def particle_step(self):
         ctas = min(self.ntiles, self.num_sms * self.cfg.ctas_per_sm)
         _lib.call("pxrb_tiled_particle_step", self.job_dev.data_ptr(), self.order, self.prec,
                   self.work.data_ptr(), self.ntiles, None, self.ctr.data_ptr(),
                   self.cfg.threads, ctas, self.smem, _stream())
+        self.launches += 1
 
     def push_b(self, frac=0.5):
         _lib.call("pxrb_tiled_push_b", self.job_dev.data_ptr(), 1, self.prec,
                   self.cell_off.data_ptr(), self.total_cells, frac, _stream())
+        self.launches += 1
 
     def push_e(self, zero_j=True):
         _lib.call("pxrb_tiled_push_e", self.job_dev.data_ptr(), 1, self.prec,
                   self.cell_off.data_ptr(), self.total_cells, int(zero_j), _stream())
+        self.launches += 1
 
-    def step(self, nsteps=1, keep_j=False):
+    def step(self, nsteps=1, keep_j=False, events=None):
         """nsteps PIC steps.  keep_j: leave the last step's J in place (it is
-        otherwise consumed by the E push); the next step clears it."""
+        otherwise consumed by the E push); the next step clears it.  events:
+        a (start, end) pair of CUDA events recorded around the particle
+        kernel (nsteps = 1)."""
         for s in range(nsteps):
             if getattr(self, "_j_dirty", False):
                 for t in self.J:
                     t.zero_()
                 self._j_dirty = False
+            if events is not None:
+                events[0].record(torch.cuda.current_stream())
             self.particle_step()
+            if events is not None:
+                events[1].record(torch.cuda.current_stream())
             self.push_b(0.5)
             last = s == nsteps - 1
             self.push_e(zero_j=not (keep_j and last))
@@ -277,15 +286,19 @@ class TiledSim:
                 self.sort()
 
     # ----------------------------------------------------------- diagnostics
-    def diagnostics(self):
-        """FP64 energies and Gauss-law residual of the current state."""
+    def diagnostics(self, gauss=True, to_host=True):
+        """FP64 energies and (gauss=True) the Gauss-law residual of the current
+        state; to_host=False leaves the 9 values in self.diag_out (device)."""
         n_scr = _lib.query("pxrb_tiled_diag_scratch", self._jp())
         if getattr(self, "_scratch", None) is None or self._scratch.numel() < n_scr:
             self._scratch = torch.zeros(n_scr, dtype=torch.float64, device=self.device)
-        self._pull_job()
-        _lib.call("pxrb_tiled_diagnostics", self._jp(), self.rho.data_ptr(),
-                  self._scratch.data_ptr(), self._scratch.numel(), self.diag_out.data_ptr(),
-                  _stream())
+        if gauss:
+            self._pull_job()     # rho deposition reads the current particle arrays
+        _lib.call("pxrb_tiled_diagnostics", self._jp(),
+                  self.rho.data_ptr() if gauss else None, self._scratch.data_ptr(),
+                  self._scratch.numel(), self.diag_out.data_ptr(), _stream())
+        if not to_host:
+            return self.diag_out
         o = self.diag_out.cpu().tolist()
         return {"kinetic": o[0], "ex": o[1], "ey": o[2], "ez": o[3], "bx": o[4], "by": o[5],
                 "bz": o[6], "gauss_norm": o[7], "rho_norm": o[8], "field": sum(o[1:7]),
