@@ -64,30 +64,45 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+    """nvidia-smi sampling (every 100 ms) of the SM clock and the throttle
+    reasons of this rank's GPU while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, dev_index):
         import torch
         self.proc = None
+        self.index = None
+        os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
         self.out = os.path.join(ROOT, "gpurun_out", f"clocks_rank{dev_index}.csv")
         try:
-            bus = torch.cuda.get_device_properties(dev_index).pci_bus_id
-        except Exception:
-            bus = str(dev_index)
-        self.bus = bus
+            pr = torch.cuda.get_device_properties(dev_index)
+            want = (int(pr.pci_domain_id), int(pr.pci_bus_id), int(pr.pci_device_id))
+            r = subprocess.run(["nvidia-smi", "--query-gpu=index,pci.bus_id",
+                                "--format=csv,noheader"], capture_output=True, text=True,
+                               timeout=20)
+            for line in r.stdout.splitlines():
+                idx, pb = (p.strip() for p in line.split(",", 1))
+                dom, bus, devfn = pb.split(":")
+                if (int(dom, 16), int(bus, 16), int(devfn.split(".")[0], 16)) == want:
+                    self.index = idx
+        except Exception as e:
+            print(f"clock sampler: {e!r}", file=sys.stderr)
+            self.index = None
+        if self.index is None:
+            print(f"clock sampler: no nvidia-smi index for this GPU", file=sys.stderr)
 
     def start(self):
-        os.makedirs(os.path.dirname(self.out), exist_ok=True)
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-        try:
-            self.fh = open(self.out, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.bus, f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=self.fh, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+        if self.index is None:
+            return
+        self.fh = open(self.out, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", self.index,
+                                      f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "100"],
+                                     stdout=self.fh, stderr=subprocess.DEVNULL)
 
     def stop(self):
         if self.proc is None:
@@ -98,21 +113,24 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.fh.close()
-        rows = []
+        sm, mx, reasons = [], [], set()
         with open(self.out) as f:
             for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 8:
-                    rows.append(parts)
-        if not rows:
+                p = [v.strip() for v in line.split(",")]
+                if len(p) < 7:
+                    continue
+                try:
+                    sm.append(float(p[0]))
+                    mx.append(float(p[1]))
+                except ValueError:
+                    continue
+                for name, v in zip(self.NAMES, p[3:7]):
+                    if v == "Active":
+                        reasons.add(name)
+        if not sm:
             return None
-        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
 
 
 def _dist():
@@ -208,7 +226,7 @@ def run_ours(args):
     wl = WORKLOADS[args.workload]
     prec = 0 if args.precision == "fp32" else 1
     cfg = TiledConfig(tile=wl["tile"], sort_interval=wl["sort_interval"], drift=1,
-                      threads=args.threads, ctas_per_sm=args.ctas_per_sm)
+                      threads=args.threads, ctas_per_sm=args.ctas_per_sm, acc=args.acc)
     st = thermal_plasma(wl["n"], wl["ppc"], wl["sigma"], seed=1234 + rank, device="cuda")
     N = st.np
     sim = TiledSim(wl["n"], order=wl["order"], pusher=wl["pusher"], precision=args.precision,
@@ -287,7 +305,7 @@ def run_ours(args):
                              f"{N * 32 / 1e9:.1f} GB per GPU), no flush",
                        "tuning": {"tile": list(wl["tile"]), "drift": cfg.drift,
                                   "threads": cfg.threads, "ctas_per_sm": cfg.ctas_per_sm,
-                                  "sort_interval": cfg.sort_interval}},
+                                  "sort_interval": cfg.sort_interval, "acc": cfg.acc}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": f"k_tiled_step<{'float' if prec == 0 else 'double'},"
@@ -387,6 +405,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--ctas-per-sm", type=int, default=2)
+    ap.add_argument("--acc", type=int, default=2, help="FP32 current accumulator mode")
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--skip-e2e", action="store_true")

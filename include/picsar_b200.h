@@ -203,7 +203,7 @@ typedef struct pxrb_tiled_job {
   int32_t pusher;            /* 0 Boris (+ set_gamma), 1 Vay */
   int32_t drift;             /* window margin (cells) around each tile */
   int32_t prec;              /* 0 float, 1 double */
-  int32_t pad0;
+  int32_t pitch_y;           /* allocated y extent of the E/B arrays */
   int64_t np;                /* particles */
   double dx, dy, dz, dt, q, m, clight, mu0, eps0, xmin, ymin, zmin;
   void *ex, *ey, *ez, *bx, *by, *bz;        /* guarded, engine precision */
@@ -219,8 +219,19 @@ typedef struct pxrb_tiled_job {
   double* ke_tile;                          /* ntiles: kinetic energy per tile */
   int32_t* counters;                        /* [0] particles on the slow path,
                                                [1] error flag */
+  int32_t* cell_cnt;                        /* sort scratch: ntiles * tile^3 */
+  int32_t* rank_b;                          /* sort scratch: np */
 } pxrb_tiled_job;
 
+/* Tile shapes: cubic tiles of edge tx = ty = tz = `tile` in {4, 8} with window
+ * margin `drift` in {0, 1, 2} (8) or {0, 1} (4); the E/B arrays are allocated
+ * with extents (pitch_x >= ntx*tile + 2g, pitch_y >= nty*tile + 2g,
+ * ntz*tile + 2g) so that every tile window fits.  g >= drift + 2.
+ * `acc` selects the shared-memory accumulator of a tile's current:
+ * 0 FP32 atomics, 1 int32 fixed point, 2 64-bit fixed point held in two
+ * native int32 words (default of the FP32 engine), 3 FP64 (FP64 engine).  The
+ * fixed-point scales are bounded per tile from the tile's particle weights,
+ * momenta, cell occupancy and fields, so no overflow is possible. */
 /* Fused per-step particle kernel of the tiled engine: energy-conserving
  * gather (l_lower_order_in_v), Boris or Vay push, position push, periodic
  * wrap, and Esirkepov deposition from the exact old position into J (+=).
@@ -236,17 +247,18 @@ typedef struct pxrb_tiled_job {
  * the call; threads: CTA size, multiple of 32, <= 256; smem: dynamic shared
  * memory bytes, >= pxrb_tiled_smem_bytes() of the largest tile window. */
 int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int32_t prec,
-                             const int32_t* work, int32_t nwork, const int32_t* nwork_dev,
-                             int32_t* ctr, int32_t threads, int32_t ctas, int64_t smem,
-                             void* stream);
+                             int32_t tile, int32_t drift, int32_t acc, const int32_t* work,
+                             int32_t nwork,
+                             const int32_t* nwork_dev, int32_t* ctr, int32_t threads,
+                             int32_t ctas, int64_t smem, void* stream);
 
 /* sizeof(pxrb_tiled_job), for bindings that mirror the struct. */
 int64_t pxrb_tiled_job_size(void);
 
 /* Dynamic shared memory the particle kernel needs for a tile shape, order,
  * window margin and precision (host function, no GPU work). */
-int64_t pxrb_tiled_smem_bytes(int32_t order, int32_t prec, int32_t tx, int32_t ty,
-                              int32_t tz, int32_t drift);
+int64_t pxrb_tiled_smem_bytes(int32_t order, int32_t prec, int32_t acc, int32_t tx,
+                              int32_t ty, int32_t tz, int32_t drift);
 
 /* Yee steps on the engine layout, every job in one launch (yee.F90:1258-1347
  * and :637-740; periodic guard images written by the same kernel).
@@ -263,9 +275,14 @@ int pxrb_tiled_push_e(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t pre
 
 /* Counting sort of one job's particles by cell tile: the B200 form of
  * pxr_particle_sorting (src/housekeeping/sorting.F90:67-361) with the tile of
- * the particle's cell as key; order inside a tile is unspecified.  Rebuilds
- * tile_off and swaps, in the DEVICE descriptor, the particle arrays with
- * their *_b buffers.  job_host: host copy (sizes, tile_cnt, tile_off). */
+ * the particle's cell as key.  Inside a tile the particles are laid out
+ * round-robin over the tile's cells (every cell's first particle, then every
+ * cell's second, ...), the cells ranked so that 32 consecutive ones fall in
+ * distinct shared-memory banks of the tile window: a warp of the particle
+ * kernel then touches 32 different cells without bank conflicts.  Rebuilds
+ * tile_off; the particle arrays keep their addresses (the *_b buffers, and
+ * cell_cnt / rank_b, are scratch).  job_host: host copy (sizes and pointers);
+ * job_dev: the device copy the kernels read. */
 int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, void* stream);
 
 /* Conversions between PICSAR's particle arrays (absolute FP64 positions,

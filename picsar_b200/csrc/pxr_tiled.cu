@@ -20,437 +20,16 @@
 
 #include <cub/block/block_scan.cuh>
 
+namespace pxrt {
+int launch_order1(int, int, int, int, const pxrb_tiled_job*, const int2*, int, const int*, int*, int, int, size_t, cudaStream_t);
+int launch_order2(int, int, int, int, const pxrb_tiled_job*, const int2*, int, const int*, int*, int, int, size_t, cudaStream_t);
+int launch_order3(int, int, int, int, const pxrb_tiled_job*, const int2*, int, const int*, int*, int, int, size_t, cudaStream_t);
+}  // namespace pxrt
+
+#include "pxr_tiled_kernel.cuh"
+
 namespace {
-
-typedef pxrb_tiled_job Job;
-
-// ---------------------------------------------------------------------------
-// packed cell index: x | y << 11 | z << 22
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void unpack_cell(uint32_t c, int& i, int& j, int& k) {
-  i = (int)(c & 2047u);
-  j = (int)((c >> 11) & 2047u);
-  k = (int)(c >> 22);
-}
-__device__ __forceinline__ uint32_t pack_cell(int i, int j, int k) {
-  return (uint32_t)i | ((uint32_t)j << 11) | ((uint32_t)k << 22);
-}
-
-// Reach of the gather and deposition stencils around a particle's cell c:
-// nodes [c - L, c + H] (also covers the Esirkepov box when the cell changes
-// by one, which is accounted for by the window margin).
-template <int ORDER> struct Reach {
-  static constexpr int L = ORDER == 1 ? 0 : 1;
-  static constexpr int H = ORDER == 1 ? 1 : 2;
-};
-
-// ---------------------------------------------------------------------------
-// Shapes from (cell, offset): x = c + o with o in [0,1).  r0 is the first
-// support node relative to c.  Same formulas as NodeShape/StagShape, with
-// floor(x) = c and nint(x) = c + (o >= 1/2) for x >= 0.
-// ---------------------------------------------------------------------------
-template <int ORDER, typename R> struct NodeCO {
-  static constexpr int N = ORDER + 1;
-  int r0;
-  R s[N];
-  __device__ __forceinline__ void set(R o) {
-    if (ORDER == 1) {
-      r0 = 0; s[0] = (R)1 - o; s[1] = o;
-    } else if (ORDER == 2) {
-      int r = o >= (R)0.5 ? 1 : 0;
-      R xi = o - (R)r, xs = xi * xi;
-      r0 = r - 1;
-      s[0] = (R)0.5 * ((R)0.5 - xi) * ((R)0.5 - xi);
-      s[1] = (R)0.75 - xs;
-      s[2] = (R)0.5 * ((R)0.5 + xi) * ((R)0.5 + xi);
-    } else {
-      R xi = o, ox = (R)1 - xi, xs = xi * xi, oxs = ox * ox;
-      r0 = -1;
-      s[0] = (R)(1.0 / 6.0) * oxs * ox;
-      s[1] = (R)(2.0 / 3.0) - xs * ((R)1 - xi * (R)0.5);
-      s[2] = (R)(2.0 / 3.0) - oxs * ((R)1 - ox * (R)0.5);
-      s[3] = (R)(1.0 / 6.0) * xs * xi;
-    }
-  }
-};
-
-template <int ORDER, typename R> struct StagCO {
-  static constexpr int N = ORDER;
-  int r0;
-  R s[N];
-  __device__ __forceinline__ void set(R o) {
-    if (ORDER == 1) {
-      r0 = 0; s[0] = (R)1;
-    } else if (ORDER == 2) {
-      int j0 = o >= (R)0.5 ? 0 : -1;
-      R xi = o - (R)0.5 - (R)j0;
-      r0 = j0; s[0] = (R)1 - xi; s[1] = xi;
-    } else {
-      R xi = o - (R)0.5, xs = xi * xi;
-      r0 = -1;
-      s[0] = (R)0.5 * ((R)0.5 - xi) * ((R)0.5 - xi);
-      s[1] = (R)0.75 - xs;
-      s[2] = (R)0.5 * ((R)0.5 + xi) * ((R)0.5 + xi);
-    }
-  }
-};
-
-// Esirkepov node index (relative to c) and in-cell variable of a position
-template <int ORDER, typename R>
-__device__ __forceinline__ void esir_node(R o, int& r, R& xi) {
-  if (ORDER == 2) {
-    r = o >= (R)0.5 ? 1 : 0;
-    xi = o - (R)r;
-  } else {
-    r = 0;
-    xi = o;
-  }
-}
-
-// Field accessor: either a shared-memory window or the global guarded arrays.
-template <typename R> struct FieldView {
-  const R* p;       // element (0,0,0) of the view
-  int sy, sz;       // strides
-  __device__ __forceinline__ R at(int i, int j, int k) const { return p[i + sy * j + sz * k]; }
-};
-
-template <int NA, int NB, int NC, typename R>
-__device__ __forceinline__ R gsum(const FieldView<R>& f, int ia, const R* sa, int ib,
-                                  const R* sb, int ic, const R* sc) {
-  R out = (R)0;
-#pragma unroll
-  for (int c = 0; c < NC; ++c) {
-    R a = (R)0;
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {
-      R r = (R)0;
-#pragma unroll
-      for (int t = 0; t < NA; ++t) r = r + sa[t] * f.at(ia + t, ib + b, ic + c);
-      a = a + r * sb[b];
-    }
-    out = out + a * sc[c];
-  }
-  return out;
-}
-
-// Gather E and B at a particle whose cell is (ci, cj, ck) in the view's
-// coordinates.
-template <int ORDER, typename R>
-__device__ __forceinline__ void gather6(const FieldView<R>* F, int ci, int cj, int ck, R ox,
-                                        R oy, R oz, R* eb) {
-  NodeCO<ORDER, R> nx, ny, nz;
-  StagCO<ORDER, R> sx, sy, sz;
-  nx.set(ox); ny.set(oy); nz.set(oz);
-  sx.set(ox); sy.set(oy); sz.set(oz);
-  constexpr int N = ORDER + 1, S = ORDER;
-  eb[0] = gsum<S, N, N>(F[0], ci + sx.r0, sx.s, cj + ny.r0, ny.s, ck + nz.r0, nz.s);
-  eb[1] = gsum<N, S, N>(F[1], ci + nx.r0, nx.s, cj + sy.r0, sy.s, ck + nz.r0, nz.s);
-  eb[2] = gsum<N, N, S>(F[2], ci + nx.r0, nx.s, cj + ny.r0, ny.s, ck + sz.r0, sz.s);
-  eb[3] = gsum<N, S, S>(F[3], ci + nx.r0, nx.s, cj + sy.r0, sy.s, ck + sz.r0, sz.s);
-  eb[4] = gsum<S, N, S>(F[4], ci + sx.r0, sx.s, cj + ny.r0, ny.s, ck + sz.r0, sz.s);
-  eb[5] = gsum<S, S, N>(F[5], ci + sx.r0, sx.s, cj + sy.r0, sy.s, ck + nz.r0, nz.s);
-}
-
-// Accumulator target for the deposition: shared window (atomicAdd on A) or
-// the global periodic FP64 grid.
-template <typename A> struct SmemAcc {
-  A* p;
-  int sy, sz;
-  __device__ __forceinline__ void add(int i, int j, int k, A v) const {
-    atomicAdd(p + i + sy * j + sz * k, v);
-  }
-};
-struct GlobAcc {
-  double* p;
-  int nx, ny, nz;
-  __device__ __forceinline__ static int wrap(int i, int n) {
-    return i < 0 ? i + n : (i >= n ? i - n : i);
-  }
-  __device__ __forceinline__ void add(int i, int j, int k, double v) const {
-    i = wrap(i, nx); j = wrap(j, ny); k = wrap(k, nz);
-    atomicAdd(p + i + (i64)nx * (j + (i64)ny * k), v);
-  }
-};
-
-// Esirkepov current of one particle into three accumulators, box in the
-// accumulator's coordinates.  Same arithmetic as esirkepov_3d.F90 (prefix
-// sums of W along x for Jx, y for Jy, z for Jz).
-template <int ORDER, typename R, typename ACC, typename AV>
-__device__ __forceinline__ void esirkepov_dep(const EsirAxis<ORDER, R>& X,
-                                              const EsirAxis<ORDER, R>& Y,
-                                              const EsirAxis<ORDER, R>& Z, R wqx, R wqy, R wqz,
-                                              const ACC& jx, const ACC& jy, const ACC& jz) {
-  constexpr int M = ORDER + 2;
-  const R onethird = (R)(1.0 / 3.0);
-#pragma unroll
-  for (int k = 0; k < M; ++k) {
-    if (k >= Z.n) continue;
-    R dsz = Z.s1[k] - Z.s0[k];
-#pragma unroll
-    for (int j = 0; j < M; ++j) {
-      if (j >= Y.n) continue;
-      R dsy = Y.s1[j] - Y.s0[j];
-      R fyz = (Y.s0[j] + (R)0.5 * dsy) * Z.s0[k] + ((R)0.5 * Y.s0[j] + onethird * dsy) * dsz;
-      R acc = (R)0;
-#pragma unroll
-      for (int i = 0; i < M - 1; ++i) {
-        if (i >= X.n - 1) continue;
-        acc = acc + wqx * (X.s1[i] - X.s0[i]) * fyz;
-        jx.add(X.i0 + i, Y.i0 + j, Z.i0 + k, (AV)acc);
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < M; ++k) {
-    if (k >= Z.n) continue;
-    R dsz = Z.s1[k] - Z.s0[k];
-#pragma unroll
-    for (int i = 0; i < M; ++i) {
-      if (i >= X.n) continue;
-      R dsx = X.s1[i] - X.s0[i];
-      R fzx = (Z.s0[k] + (R)0.5 * dsz) * X.s0[i] + ((R)0.5 * Z.s0[k] + onethird * dsz) * dsx;
-      R acc = (R)0;
-#pragma unroll
-      for (int j = 0; j < M - 1; ++j) {
-        if (j >= Y.n - 1) continue;
-        acc = acc + wqy * (Y.s1[j] - Y.s0[j]) * fzx;
-        jy.add(X.i0 + i, Y.i0 + j, Z.i0 + k, (AV)acc);
-      }
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < M; ++j) {
-    if (j >= Y.n) continue;
-    R dsy = Y.s1[j] - Y.s0[j];
-#pragma unroll
-    for (int i = 0; i < M; ++i) {
-      if (i >= X.n) continue;
-      R dsx = X.s1[i] - X.s0[i];
-      R fxy = (X.s0[i] + (R)0.5 * dsx) * Y.s0[j] + ((R)0.5 * X.s0[i] + onethird * dsx) * dsy;
-      R acc = (R)0;
-#pragma unroll
-      for (int k = 0; k < M - 1; ++k) {
-        if (k >= Z.n - 1) continue;
-        acc = acc + wqz * (Z.s1[k] - Z.s0[k]) * fxy;
-        jz.add(X.i0 + i, Y.i0 + j, Z.i0 + k, (AV)acc);
-      }
-    }
-  }
-}
-
-// Shared-memory accumulator type: FP32 window for the mixed engine, FP64 for
-// the FP64 engine.
-template <typename R> struct AccT { typedef R type; };
-
-template <typename R>
-__device__ __forceinline__ void cell_step(R& o, int& c, R du) {
-  // o + du, split into cell shift and offset in [0,1)
-  R on = o + du;
-  R fl = floor(on);
-  int s = (int)fl;
-  R of = on - fl;
-  if (of >= (R)1) { of = of - (R)1; s += 1; }
-  o = of;
-  c += s;
-}
-
-template <typename R> __device__ __forceinline__ R rsqrt_(R x);
-template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return 1.0f / sqrtf(x); }
-template <> __device__ __forceinline__ double rsqrt_<double>(double x) { return 1.0 / sqrt(x); }
-
-constexpr int MAX_THREADS = 256;
-
-// ---------------------------------------------------------------------------
-// The fused particle kernel (persistent CTAs pulling (job, tile) items).
-// ---------------------------------------------------------------------------
-template <typename R, int ORDER>
-__global__ void __launch_bounds__(MAX_THREADS)
-    k_tiled_step(const Job* __restrict__ jobs, const int2* __restrict__ work, int nwork,
-                 const int* __restrict__ nwork_dev, int* ctr) {
-  typedef typename AccT<R>::type A;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ Job sj;
-  __shared__ int s_item;
-  __shared__ double s_red[MAX_THREADS / 32];
-  constexpr int L = Reach<ORDER>::L, H = Reach<ORDER>::H;
-
-  if (nwork_dev) nwork = min(nwork, *nwork_dev);
-  for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(ctr, 1);
-    __syncthreads();
-    const int item = s_item;
-    if (item >= nwork) break;
-    const int2 wk = work[item];
-    // job descriptor into shared memory
-    {
-      const int nw = (int)(sizeof(Job) / sizeof(int));
-      const int* src = reinterpret_cast<const int*>(jobs + wk.x);
-      int* dst = reinterpret_cast<int*>(&sj);
-      for (int t = threadIdx.x; t < nw; t += blockDim.x) dst[t] = src[t];
-    }
-    __syncthreads();
-    const int nx = sj.nx, ny = sj.ny, nz = sj.nz, G = sj.g, D = sj.drift;
-    const int tile = wk.y;
-    const int ti = tile % sj.ntx, tj = (tile / sj.ntx) % sj.nty, tk = tile / (sj.ntx * sj.nty);
-    const int c0x = ti * sj.tx, c0y = tj * sj.ty, c0z = tk * sj.tz;
-    const int tex = min(sj.tx, nx - c0x), tey = min(sj.ty, ny - c0y), tez = min(sj.tz, nz - c0z);
-    const int Wx = tex + 2 * D + L + H, Wy = tey + 2 * D + L + H, Wz = tez + 2 * D + L + H;
-    const int wox = c0x - D - L, woy = c0y - D - L, woz = c0z - D - L;
-    const int V = Wx * Wy * Wz;
-    R* Fs = reinterpret_cast<R*>(smem_raw);
-    A* Js = reinterpret_cast<A*>(smem_raw + (size_t)6 * V * sizeof(R));
-    // ---- stage E/B window (guarded global arrays: no wrap needed) -------
-    const int pitch = sj.pitch_x, NYg = ny + 2 * G;
-    const R* gF[6] = {(const R*)sj.ex, (const R*)sj.ey, (const R*)sj.ez,
-                      (const R*)sj.bx, (const R*)sj.by, (const R*)sj.bz};
-    for (int e = threadIdx.x; e < 6 * V; e += blockDim.x) {
-      int comp = e / V, r = e - comp * V;
-      int a = r % Wx, rb = r / Wx, b = rb % Wy, c = rb / Wy;
-      i64 gidx = (i64)(wox + a + G) + (i64)pitch * ((woy + b + G) + (i64)NYg * (woz + c + G));
-      Fs[e] = __ldg(gF[comp] + gidx);
-    }
-    for (int e = threadIdx.x; e < 3 * V; e += blockDim.x) Js[e] = (A)0;
-    __syncthreads();
-
-    FieldView<R> FW[6], FG[6];
-    for (int c = 0; c < 6; ++c) {
-      FW[c].p = Fs + c * V; FW[c].sy = Wx; FW[c].sz = Wx * Wy;
-      FG[c].p = gF[c] + (G + (i64)pitch * (G + (i64)NYg * G));
-      FG[c].sy = pitch; FG[c].sz = pitch * NYg;
-    }
-    SmemAcc<A> JW[3];
-    for (int c = 0; c < 3; ++c) { JW[c].p = Js + c * V; JW[c].sy = Wx; JW[c].sz = Wx * Wy; }
-    GlobAcc JG[3];
-    JG[0].p = sj.jx; JG[1].p = sj.jy; JG[2].p = sj.jz;
-    for (int c = 0; c < 3; ++c) { JG[c].nx = nx; JG[c].ny = ny; JG[c].nz = nz; }
-
-    const R dtdx = (R)(sj.dt / sj.dx), dtdy = (R)(sj.dt / sj.dy), dtdz = (R)(sj.dt / sj.dz);
-    const R clghtisq = (R)(1.0 / (sj.clight * sj.clight));
-    const R cst_b = (R)(sj.q * sj.dt * 0.5 / sj.m), cst_v = (R)(sj.q * sj.dt / sj.m);
-    const R invc = (R)(1.0 / sj.clight);
-    const double invdtdx = 1.0 / (sj.dt * sj.dy * sj.dz), invdtdy = 1.0 / (sj.dt * sj.dx * sj.dz),
-                 invdtdz = 1.0 / (sj.dt * sj.dx * sj.dy);
-    const bool vay = sj.pusher == 1;
-    uint32_t* cellp = sj.cell;
-    R *oxp = (R*)sj.ox, *oyp = (R*)sj.oy, *ozp = (R*)sj.oz;
-    R *uxp = (R*)sj.ux, *uyp = (R*)sj.uy, *uzp = (R*)sj.uz;
-    const R* wp = (const R*)sj.w;
-    const int pbeg = sj.tile_off[tile], pend = sj.tile_off[tile + 1];
-    double ke = 0.0;
-    int nslow = 0, bad = 0;
-
-    for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
-      int ci, cj, ck;
-      unpack_cell(cellp[ip], ci, cj, ck);
-      R ox = oxp[ip], oy = oyp[ip], oz = ozp[ip];
-      R ux = uxp[ip], uy = uyp[ip], uz = uzp[ip];
-      const R wgt = wp[ip];
-      // tile-relative cell, unwrapped to the nearest periodic image
-      int vx = ci - c0x, vy = cj - c0y, vz = ck - c0z;
-      if (vx > tex - 1 + D) vx -= nx; else if (vx < -D) vx += nx;
-      if (vy > tey - 1 + D) vy -= ny; else if (vy < -D) vy += ny;
-      if (vz > tez - 1 + D) vz -= nz; else if (vz < -D) vz += nz;
-      const bool in_old = vx >= -D && vx <= tex - 1 + D && vy >= -D && vy <= tey - 1 + D &&
-                          vz >= -D && vz <= tez - 1 + D;
-      // ---- gather ----------------------------------------------------------
-      R eb[6];
-      if (in_old) {
-        gather6<ORDER, R>(FW, vx + D + L, vy + D + L, vz + D + L, ox, oy, oz, eb);
-      } else {
-        gather6<ORDER, R>(FG, ci, cj, ck, ox, oy, oz, eb);
-      }
-      // ---- push ------------------------------------------------------------
-      R gi;
-      if (vay) {
-        gi = rsqrt_<R>((R)1 + (ux * ux + uy * uy + uz * uz) * clghtisq);
-        vay_push(ux, uy, uz, gi, eb[0], eb[1], eb[2], eb[3], eb[4], eb[5], cst_v, invc, clghtisq);
-      } else {
-        boris_push(ux, uy, uz, gi, eb[0], eb[1], eb[2], eb[3], eb[4], eb[5], cst_b, clghtisq);
-        set_gamma(ux, uy, uz, gi, clghtisq);
-      }
-      // ---- position: exact old (c, o), new (c', o') -------------------------
-      R nox = ox, noy = oy, noz = oz;
-      int ncx = 0, ncy = 0, ncz = 0;   // cell shift
-      cell_step(nox, ncx, ux * gi * dtdx);
-      cell_step(noy, ncy, uy * gi * dtdy);
-      cell_step(noz, ncz, uz * gi * dtdz);
-      // ---- deposition ------------------------------------------------------
-      int r0, r1;
-      R xi0, xi1;
-      EsirAxis<ORDER, R> EX, EY, EZ;
-      bool ok = true;
-      const R wq = (R)(sj.q) * wgt;
-      const R wqx = wq * (R)invdtdx, wqy = wq * (R)invdtdy, wqz = wq * (R)invdtdz;
-      const bool in_new = in_old && vx + ncx >= -D && vx + ncx <= tex - 1 + D &&
-                          vy + ncy >= -D && vy + ncy <= tey - 1 + D && vz + ncz >= -D &&
-                          vz + ncz <= tez - 1 + D;
-      // cell coordinates of the old position in the accumulator's frame
-      const int bx = in_new ? vx + D + L : ci;
-      const int by = in_new ? vy + D + L : cj;
-      const int bz = in_new ? vz + D + L : ck;
-      esir_node<ORDER, R>(nox, r0, xi0);
-      esir_node<ORDER, R>(ox, r1, xi1);
-      ok = EX.set(bx + ncx + r0, xi0, bx + r1, xi1) && ok;
-      esir_node<ORDER, R>(noy, r0, xi0);
-      esir_node<ORDER, R>(oy, r1, xi1);
-      ok = EY.set(by + ncy + r0, xi0, by + r1, xi1) && ok;
-      esir_node<ORDER, R>(noz, r0, xi0);
-      esir_node<ORDER, R>(oz, r1, xi1);
-      ok = EZ.set(bz + ncz + r0, xi0, bz + r1, xi1) && ok;
-      if (!ok) bad = 1;
-      if (in_new) {
-        esirkepov_dep<ORDER, R, SmemAcc<A>, A>(EX, EY, EZ, wqx, wqy, wqz, JW[0], JW[1], JW[2]);
-      } else {
-        ++nslow;
-        esirkepov_dep<ORDER, R, GlobAcc, double>(EX, EY, EZ, wqx, wqy, wqz, JG[0], JG[1], JG[2]);
-      }
-      // ---- store -----------------------------------------------------------
-      int nci = ci + ncx, ncj = cj + ncy, nck = ck + ncz;
-      nci = nci < 0 ? nci + nx : (nci >= nx ? nci - nx : nci);
-      ncj = ncj < 0 ? ncj + ny : (ncj >= ny ? ncj - ny : ncj);
-      nck = nck < 0 ? nck + nz : (nck >= nz ? nck - nz : nck);
-      cellp[ip] = pack_cell(nci, ncj, nck);
-      oxp[ip] = nox; oyp[ip] = noy; ozp[ip] = noz;
-      uxp[ip] = ux; uyp[ip] = uy; uzp[ip] = uz;
-      // kinetic energy (gamma - 1) w, in FP64 from u
-      const double u2 = (double)ux * ux + (double)uy * uy + (double)uz * uz;
-      const double c2i = 1.0 / (sj.clight * sj.clight);
-      ke += u2 * c2i / (1.0 + sqrt(1.0 + u2 * c2i)) * (double)wgt;
-    }
-    __syncthreads();
-    // ---- flush J window (FP64 atomics, zeros skipped) ----------------------
-    {
-      double* gJ[3] = {sj.jx, sj.jy, sj.jz};
-      for (int e = threadIdx.x; e < 3 * V; e += blockDim.x) {
-        A v = Js[e];
-        if (v == (A)0) continue;
-        int comp = e / V, r = e - comp * V;
-        int a = r % Wx, rb = r / Wx, b = rb % Wy, c = rb / Wy;
-        int gi = GlobAcc::wrap(wox + a, nx), gj = GlobAcc::wrap(woy + b, ny),
-            gk = GlobAcc::wrap(woz + c, nz);
-        atomicAdd(gJ[comp] + gi + (i64)nx * (gj + (i64)ny * gk), (double)v);
-      }
-    }
-    // ---- kinetic energy of the tile (deterministic per-tile partial) -------
-    {
-      double v = ke;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-      if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
-      // counters
-      if (nslow) atomicAdd(&sj.counters[0], nslow);
-      if (bad) atomicExch(&sj.counters[1], 1);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_red[w];
-        sj.ke_tile[tile] = t * sj.m * sj.clight * sj.clight;
-      }
-    }
-    __syncthreads();
-  }
-}
-
+using namespace pxrt;
 // ---------------------------------------------------------------------------
 // Yee on the guarded engine layout, all jobs in one launch.  Thread = cell.
 // cell_off[j]: start of job j in the flat cell index space (multiple of the
@@ -494,7 +73,7 @@ __global__ void __launch_bounds__(YEE_TPB)
   const int nx = J.nx, ny = J.ny, nz = J.nz;
   if (lid >= (int64_t)nx * ny * nz) return;
   const int i = (int)(lid % nx), j = (int)((lid / nx) % ny), k = (int)(lid / ((int64_t)nx * ny));
-  const int G = J.g, pitch = J.pitch_x, NYg = ny + 2 * G;
+  const int G = J.g, pitch = J.pitch_x, NYg = J.pitch_y;
   const i64 sy = pitch, sz = (i64)pitch * NYg;
   const i64 c = (i + G) + sy * (j + G) + sz * (k + G);
   const R* ex = (const R*)J.ex; const R* ey = (const R*)J.ey; const R* ez = (const R*)J.ez;
@@ -523,7 +102,7 @@ __global__ void __launch_bounds__(YEE_TPB)
   const int nx = J.nx, ny = J.ny, nz = J.nz;
   if (lid >= (int64_t)nx * ny * nz) return;
   const int i = (int)(lid % nx), j = (int)((lid / nx) % ny), k = (int)(lid / ((int64_t)nx * ny));
-  const int G = J.g, pitch = J.pitch_x, NYg = ny + 2 * G;
+  const int G = J.g, pitch = J.pitch_x, NYg = J.pitch_y;
   const i64 sy = pitch, sz = (i64)pitch * NYg;
   const i64 c = (i + G) + sy * (j + G) + sz * (k + G);
   R* ex = (R*)J.ex; R* ey = (R*)J.ey; R* ez = (R*)J.ez;
@@ -611,6 +190,19 @@ __global__ void k_sort_scatter(const Job* __restrict__ jp) {
     if (lane == leader) base = atomicAdd(&J.tile_cnt[t], __popc(peers));
     base = __shfl_sync(peers, base, leader);
     int slot = base + __popc(peers & ((1u << lane) - 1u));
+    // rank of the particle inside its cell
+    {
+      int ci, cj, ck;
+      unpack_cell(cell, ci, cj, ck);
+      const int T = J.tx;
+      const int lc = (ci % T) + T * ((cj % T) + T * (ck % T));
+      const unsigned cpeers = __match_any_sync(mask, cell);
+      const int cl = __ffs(cpeers) - 1;
+      int cbase = 0;
+      if (lane == cl) cbase = atomicAdd(&J.cell_cnt[(i64)t * T * T * T + lc], __popc(cpeers));
+      cbase = __shfl_sync(cpeers, cbase, cl);
+      J.rank_b[slot] = cbase + __popc(cpeers & ((1u << lane) - 1u));
+    }
     J.cell_b[slot] = cell;
     ox2[slot] = ox[p]; oy2[slot] = oy[p]; oz2[slot] = oz[p];
     ux2[slot] = ux[p]; uy2[slot] = uy[p]; uz2[slot] = uz[p]; w2[slot] = w[p];
@@ -618,19 +210,104 @@ __global__ void k_sort_scatter(const Job* __restrict__ jp) {
   }
 }
 
-// swap the particle arrays with the sort buffers in the device descriptor
-__global__ void k_sort_swap(Job* jp) {
-  Job& J = *jp;
-  uint32_t* c = J.cell; J.cell = J.cell_b; J.cell_b = c;
-  void* t;
-  t = J.ox; J.ox = J.ox_b; J.ox_b = t;
-  t = J.oy; J.oy = J.oy_b; J.oy_b = t;
-  t = J.oz; J.oz = J.oz_b; J.oz_b = t;
-  t = J.ux; J.ux = J.ux_b; J.ux_b = t;
-  t = J.uy; J.uy = J.uy_b; J.uy_b = t;
-  t = J.uz; J.uz = J.uz_b; J.uz_b = t;
-  t = J.w; J.w = J.w_b; J.w_b = t;
-  int32_t* q = J.pid; J.pid = J.pid_b; J.pid_b = q;
+
+// Round-robin layout of one tile (one CTA per tile): particles come tile-
+// sorted from the *_b buffers with their rank inside their cell; position =
+// (all particles of lower rank) + (cells of this rank earlier in the bank
+// order).  The bank order lists cells by (g, rho): rho = window address of the
+// cell mod 32, g = index of the cell among those with the same rho.
+constexpr int RR_TPB = 256;
+constexpr int RR_MAXR = 64;      // ranks handled per pass
+constexpr int RR_MAXC = 512;     // cells per tile (tile edge <= 8)
+
+template <typename R>
+__global__ void __launch_bounds__(RR_TPB) k_sort_rr(const Job* __restrict__ jp) {
+  const Job& J = *jp;
+  const int T = J.tx, T3 = T * T * T;
+  const int t = blockIdx.x;
+  const int b0 = J.tile_off[t], b1 = J.tile_off[t + 1];
+  if (b0 == b1) return;
+  __shared__ int cnt[RR_MAXC], key[RR_MAXC], pos_of[RR_MAXC], cell_at[RR_MAXC];
+  __shared__ unsigned bits[RR_MAXR][RR_MAXC / 32];
+  __shared__ int wpre[RR_MAXR][RR_MAXC / 32 + 1];
+  __shared__ int base_r[RR_MAXR];
+  __shared__ int s_maxr, s_carry;
+  const int L = J.order == 1 ? 0 : 1, H = J.order == 1 ? 1 : 2;
+  const int W = T + 2 * J.drift + L + H;
+  if (threadIdx.x == 0) { s_maxr = 0; s_carry = 0; }
+  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
+    cnt[lc] = J.cell_cnt[(i64)t * T3 + lc];
+    const int x = lc % T, y = (lc / T) % T, z = lc / (T * T);
+    key[lc] = (x + W * y + W * W * z) & 31;          // residue for now
+  }
+  __syncthreads();
+  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
+    const int rho = key[lc];
+    int g = 0;
+    for (int c = 0; c < lc; ++c) g += (key[c] == rho);
+    pos_of[lc] = g * 32 + rho;                        // final key, stored aside
+    atomicMax(&s_maxr, cnt[lc]);
+  }
+  __syncthreads();
+  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) key[lc] = pos_of[lc];
+  __syncthreads();
+  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
+    const int k = key[lc];
+    int q = 0;
+    for (int c = 0; c < T3; ++c) q += (key[c] < k);
+    pos_of[lc] = q;
+    cell_at[q] = lc;
+  }
+  __syncthreads();
+  const int nw = (T3 + 31) / 32;
+  const int maxr = s_maxr;
+  const R *ox = (const R*)J.ox_b, *oy = (const R*)J.oy_b, *oz = (const R*)J.oz_b;
+  const R *ux = (const R*)J.ux_b, *uy = (const R*)J.uy_b, *uz = (const R*)J.uz_b;
+  const R* w = (const R*)J.w_b;
+  R *ox2 = (R*)J.ox, *oy2 = (R*)J.oy, *oz2 = (R*)J.oz;
+  R *ux2 = (R*)J.ux, *uy2 = (R*)J.uy, *uz2 = (R*)J.uz, *w2 = (R*)J.w;
+  const int ti = t % J.ntx, tj = (t / J.ntx) % J.nty, tk = t / (J.ntx * J.nty);
+  for (int r0 = 0; r0 < maxr; r0 += RR_MAXR) {
+    const int nr = min(RR_MAXR, maxr - r0);
+    for (int e = threadIdx.x; e < nr * nw; e += blockDim.x) {
+      const int i = e / nw, wd = e % nw;
+      unsigned m = 0;
+      for (int b = 0; b < 32; ++b) {
+        const int q = wd * 32 + b;
+        if (q < T3 && cnt[cell_at[q]] > r0 + i) m |= 1u << b;
+      }
+      bits[i][wd] = m;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+      int acc = 0;
+      for (int wd = 0; wd < nw; ++wd) { wpre[i][wd] = acc; acc += __popc(bits[i][wd]); }
+      wpre[i][nw] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int c = s_carry;
+      for (int i = 0; i < nr; ++i) { base_r[i] = c; c += wpre[i][nw]; }
+      s_carry = c;
+    }
+    __syncthreads();
+    for (int p = b0 + threadIdx.x; p < b1; p += blockDim.x) {
+      const int r = J.rank_b[p];
+      if (r < r0 || r >= r0 + nr) continue;
+      const uint32_t cell = J.cell_b[p];
+      int ci, cj, ck;
+      unpack_cell(cell, ci, cj, ck);
+      const int lc = (ci - ti * T) + T * ((cj - tj * T) + T * (ck - tk * T));
+      const int q = pos_of[lc], i = r - r0;
+      const int pos = base_r[i] + wpre[i][q >> 5] + __popc(bits[i][q >> 5] & ((1u << (q & 31)) - 1u));
+      const int d = b0 + pos;
+      J.cell[d] = cell;
+      ox2[d] = ox[p]; oy2[d] = oy[p]; oz2[d] = oz[p];
+      ux2[d] = ux[p]; uy2[d] = uy[p]; uz2[d] = uz[p]; w2[d] = w[p];
+      if (J.pid) J.pid[d] = J.pid_b[p];
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -687,7 +364,7 @@ __global__ void k_field_xfer(Job J, int which, double* f, int ng, int dir) {
   const int nx = J.nx, ny = J.ny, nz = J.nz, G = J.g;
   if (which < 6) {
     R* e = (R*)((&J.ex)[which]);
-    const int ex_ = nx + 2 * G, ey_ = ny + 2 * G, ez_ = nz + 2 * G;
+    const int ex_ = nx + 2 * G, ey_ = ny + 2 * G, ez_ = nz + 2 * G, py = J.pitch_y;
     const i64 total = (i64)ex_ * ey_ * ez_;
     const int sx = nx + 1 + 2 * ng, sy = ny + 1 + 2 * ng;
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < total;
@@ -695,7 +372,7 @@ __global__ void k_field_xfer(Job J, int which, double* f, int ng, int dir) {
       int a = (int)(t % ex_), b = (int)((t / ex_) % ey_), c = (int)(t / ((i64)ex_ * ey_));
       int i = a - G, j = b - G, k = c - G;
       int pi = ((i % nx) + nx) % nx, pj = ((j % ny) + ny) % ny, pk = ((k % nz) + nz) % nz;
-      i64 e_idx = a + (i64)J.pitch_x * (b + (i64)ey_ * c);
+      i64 e_idx = a + (i64)J.pitch_x * (b + (i64)py * c);
       if (dir == 0) {
         e[e_idx] = (R)f[(pi + ng) + (i64)sx * ((pj + ng) + (i64)sy * (pk + ng))];
       } else if (i >= -ng && i <= nx + ng && j >= -ng && j <= ny + ng && k >= -ng &&
@@ -712,7 +389,7 @@ __global__ void k_field_xfer(Job J, int which, double* f, int ng, int dir) {
         int i = a - ng, j = b - ng, k = c - ng;
         if (i >= -G && i < nx + G && j >= -G && j < ny + G && k >= -G && k < nz + G) continue;
         int pi = ((i % nx) + nx) % nx, pj = ((j % ny) + ny) % ny, pk = ((k % nz) + nz) % nz;
-        f[t] = (double)e[(pi + G) + (i64)J.pitch_x * ((pj + G) + (i64)ey_ * (pk + G))];
+        f[t] = (double)e[(pi + G) + (i64)J.pitch_x * ((pj + G) + (i64)py * (pk + G))];
       }
     }
   } else {
@@ -767,7 +444,7 @@ constexpr int RED_TPB = 256;
 // [7] rho^2; part[q * nblocks + block]
 template <typename R>
 __global__ void __launch_bounds__(RED_TPB) k_field_sums(Job J, const double* rho, double* part) {
-  const int nx = J.nx, ny = J.ny, nz = J.nz, G = J.g, pitch = J.pitch_x, NYg = ny + 2 * G;
+  const int nx = J.nx, ny = J.ny, nz = J.nz, G = J.g, pitch = J.pitch_x, NYg = J.pitch_y;
   const i64 sy = pitch, sz = (i64)pitch * NYg;
   const i64 total = (i64)nx * ny * nz;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -839,24 +516,12 @@ int diag_blocks(const Job& J) {
 template <int ORDER>
 constexpr int reach_total() { return Reach<ORDER>::L + Reach<ORDER>::H; }
 
-int64_t smem_bytes(int order, int prec, int tx, int ty, int tz, int drift) {
+int64_t smem_bytes(int order, int prec, int acc, int tx, int ty, int tz, int drift) {
   int lh = order == 1 ? 1 : 3;
   i64 V = (i64)(tx + 2 * drift + lh) * (ty + 2 * drift + lh) * (tz + 2 * drift + lh);
   i64 r = prec ? 8 : 4;
-  return V * (6 * r + 3 * r);
-}
-
-template <typename R, int ORDER>
-int launch_step(const Job* jobs, const int2* work, int nwork, const int* nwork_dev, int* ctr,
-                int threads, int ctas, size_t smem, cudaStream_t s) {
-  auto kern = k_tiled_step<R, ORDER>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-      cudaSuccess)
-    return PXRB_EUNSUPPORTED;
-  if (cudaMemsetAsync(ctr, 0, sizeof(int), s) != cudaSuccess) return PXRB_ELAUNCH;
-  kern<<<ctas, threads, smem, s>>>(jobs, work, nwork, nwork_dev, ctr);
-  PXRB_CHECK_LAUNCH();
-  return PXRB_OK;
+  i64 a = acc == 3 ? 8 : 4, nw = acc == 2 ? 2 : 1;
+  return V * (6 * r + 3 * a * nw) + (i64)pxrt::QCAP * (3 * r + 8);
 }
 
 inline int gs_blocks(i64 n, int tpb) {
@@ -871,15 +536,16 @@ extern "C" {
 
 int64_t pxrb_tiled_job_size(void) { return (int64_t)sizeof(pxrb_tiled_job); }
 
-int64_t pxrb_tiled_smem_bytes(int32_t order, int32_t prec, int32_t tx, int32_t ty, int32_t tz,
-                              int32_t drift) {
-  return smem_bytes(order, prec, tx, ty, tz, drift);
+int64_t pxrb_tiled_smem_bytes(int32_t order, int32_t prec, int32_t acc, int32_t tx, int32_t ty,
+                              int32_t tz, int32_t drift) {
+  return smem_bytes(order, prec, acc, tx, ty, tz, drift);
 }
 
 int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int32_t prec,
-                             const int32_t* work, int32_t nwork, const int32_t* nwork_dev,
-                             int32_t* ctr, int32_t threads, int32_t ctas, int64_t smem,
-                             void* stream) {
+                             int32_t tile, int32_t drift, int32_t acc, const int32_t* work,
+                             int32_t nwork,
+                             const int32_t* nwork_dev, int32_t* ctr, int32_t threads,
+                             int32_t ctas, int64_t smem, void* stream) {
   if (!jobs_dev || !work || !ctr || nwork < 0 || smem < 0) return PXRB_EINVAL;
   if (nwork == 0) return PXRB_OK;
   if (threads < 32 || threads > MAX_THREADS || threads % 32) return PXRB_EINVAL;
@@ -887,18 +553,14 @@ int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int3
   if (ctas < 1) ctas = 1;
   cudaStream_t s = (cudaStream_t)stream;
   const int2* w2 = reinterpret_cast<const int2*>(work);
-#define PXRB_STEP(R_, O_) \
-  return launch_step<R_, O_>(jobs_dev, w2, nwork, nwork_dev, ctr, threads, ctas, (size_t)smem, s);
-  if (prec == 0) {
-    if (order == 1) { PXRB_STEP(float, 1) }
-    if (order == 2) { PXRB_STEP(float, 2) }
-    PXRB_STEP(float, 3)
-  } else {
-    if (order == 1) { PXRB_STEP(double, 1) }
-    if (order == 2) { PXRB_STEP(double, 2) }
-    PXRB_STEP(double, 3)
-  }
-#undef PXRB_STEP
+  if (order == 1)
+    return pxrt::launch_order1(prec, tile, drift, acc, jobs_dev, w2, nwork, nwork_dev, ctr,
+                               threads, ctas, (size_t)smem, s);
+  if (order == 2)
+    return pxrt::launch_order2(prec, tile, drift, acc, jobs_dev, w2, nwork, nwork_dev, ctr,
+                               threads, ctas, (size_t)smem, s);
+  return pxrt::launch_order3(prec, tile, drift, acc, jobs_dev, w2, nwork, nwork_dev, ctr,
+                             threads, ctas, (size_t)smem, s);
 }
 
 int pxrb_tiled_push_b(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
@@ -935,13 +597,22 @@ int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, voi
   cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemsetAsync(J.tile_cnt, 0, sizeof(int32_t) * (ntiles + 1), s) != cudaSuccess)
     return PXRB_ELAUNCH;
+  if (J.tx != J.ty || J.ty != J.tz || J.tx * J.tx * J.tx > RR_MAXC || !J.cell_cnt || !J.rank_b)
+    return PXRB_EINVAL;
+  if (cudaMemsetAsync(J.cell_cnt, 0, sizeof(int32_t) * (size_t)ntiles * J.tx * J.tx * J.tx, s) !=
+      cudaSuccess)
+    return PXRB_ELAUNCH;
   const int nb = gs_blocks(J.np, 256);
   if (J.np > 0) k_sort_count<<<nb, 256, 0, s>>>(job_dev);
   k_sort_scan<<<1, SCAN_TPB, 0, s>>>(job_dev);
   if (J.np > 0) {
-    if (J.prec == 0) k_sort_scatter<float><<<nb, 256, 0, s>>>(job_dev);
-    else k_sort_scatter<double><<<nb, 256, 0, s>>>(job_dev);
-    k_sort_swap<<<1, 1, 0, s>>>(job_dev);
+    if (J.prec == 0) {
+      k_sort_scatter<float><<<nb, 256, 0, s>>>(job_dev);
+      k_sort_rr<float><<<ntiles, RR_TPB, 0, s>>>(job_dev);
+    } else {
+      k_sort_scatter<double><<<nb, 256, 0, s>>>(job_dev);
+      k_sort_rr<double><<<ntiles, RR_TPB, 0, s>>>(job_dev);
+    }
   }
   PXRB_CHECK_LAUNCH();
   return PXRB_OK;

@@ -1,0 +1,809 @@
+// Device code of the tiled engine's fused particle kernel (included by the
+// per-order translation units pxr_tiled_o{1,2,3}.cu).
+#pragma once
+#include "pxr_common.cuh"
+#include "picsar_b200.h"
+
+namespace pxrt {
+
+typedef pxrb_tiled_job Job;
+
+// ---------------------------------------------------------------------------
+// packed cell index: x | y << 11 | z << 22
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void unpack_cell(uint32_t c, int& i, int& j, int& k) {
+  i = (int)(c & 2047u);
+  j = (int)((c >> 11) & 2047u);
+  k = (int)(c >> 22);
+}
+__device__ __forceinline__ uint32_t pack_cell(int i, int j, int k) {
+  return (uint32_t)i | ((uint32_t)j << 11) | ((uint32_t)k << 22);
+}
+
+// Reach of the gather and deposition stencils around a particle's cell c:
+// nodes [c - L, c + H] (also covers the Esirkepov box when the cell changes
+// by one, which is accounted for by the window margin).
+template <int ORDER> struct Reach {
+  static constexpr int L = ORDER == 1 ? 0 : 1;
+  static constexpr int H = ORDER == 1 ? 1 : 2;
+};
+
+// ---------------------------------------------------------------------------
+// Shapes from (cell, offset): x = c + o with o in [0,1).  r0 is the first
+// support node relative to c.  Same formulas as NodeShape/StagShape, with
+// floor(x) = c and nint(x) = c + (o >= 1/2) for x >= 0.
+// ---------------------------------------------------------------------------
+template <int ORDER, typename R> struct NodeCO {
+  static constexpr int N = ORDER + 1;
+  int r0;
+  R s[N];
+  __device__ __forceinline__ void set(R o) {
+    if (ORDER == 1) {
+      r0 = 0; s[0] = (R)1 - o; s[1] = o;
+    } else if (ORDER == 2) {
+      int r = o >= (R)0.5 ? 1 : 0;
+      R xi = o - (R)r, xs = xi * xi;
+      r0 = r - 1;
+      s[0] = (R)0.5 * ((R)0.5 - xi) * ((R)0.5 - xi);
+      s[1] = (R)0.75 - xs;
+      s[2] = (R)0.5 * ((R)0.5 + xi) * ((R)0.5 + xi);
+    } else {
+      R xi = o, ox = (R)1 - xi, xs = xi * xi, oxs = ox * ox;
+      r0 = -1;
+      s[0] = (R)(1.0 / 6.0) * oxs * ox;
+      s[1] = (R)(2.0 / 3.0) - xs * ((R)1 - xi * (R)0.5);
+      s[2] = (R)(2.0 / 3.0) - oxs * ((R)1 - ox * (R)0.5);
+      s[3] = (R)(1.0 / 6.0) * xs * xi;
+    }
+  }
+};
+
+template <int ORDER, typename R> struct StagCO {
+  static constexpr int N = ORDER;
+  int r0;
+  R s[N];
+  __device__ __forceinline__ void set(R o) {
+    if (ORDER == 1) {
+      r0 = 0; s[0] = (R)1;
+    } else if (ORDER == 2) {
+      int j0 = o >= (R)0.5 ? 0 : -1;
+      R xi = o - (R)0.5 - (R)j0;
+      r0 = j0; s[0] = (R)1 - xi; s[1] = xi;
+    } else {
+      R xi = o - (R)0.5, xs = xi * xi;
+      r0 = -1;
+      s[0] = (R)0.5 * ((R)0.5 - xi) * ((R)0.5 - xi);
+      s[1] = (R)0.75 - xs;
+      s[2] = (R)0.5 * ((R)0.5 + xi) * ((R)0.5 + xi);
+    }
+  }
+};
+
+// Esirkepov node index (relative to c) and in-cell variable of a position
+template <int ORDER, typename R>
+__device__ __forceinline__ void esir_node(R o, int& r, R& xi) {
+  if (ORDER == 2) {
+    r = o >= (R)0.5 ? 1 : 0;
+    xi = o - (R)r;
+  } else {
+    r = 0;
+    xi = o;
+  }
+}
+
+// Field accessor: either a shared-memory window or the global guarded arrays.
+template <typename R> struct FieldView {
+  const R* p;       // element (0,0,0) of the view
+  int sy, sz;       // strides
+  __device__ __forceinline__ R at(int i, int j, int k) const { return p[i + sy * j + sz * k]; }
+};
+
+template <int NA, int NB, int NC, typename R>
+__device__ __forceinline__ R gsum(const FieldView<R>& f, int ia, const R* sa, int ib,
+                                  const R* sb, int ic, const R* sc) {
+  R out = (R)0;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    R a = (R)0;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      R r = (R)0;
+#pragma unroll
+      for (int t = 0; t < NA; ++t) r = r + sa[t] * f.at(ia + t, ib + b, ic + c);
+      a = a + r * sb[b];
+    }
+    out = out + a * sc[c];
+  }
+  return out;
+}
+
+// Gather E and B at a particle whose cell is (ci, cj, ck) in the view's
+// coordinates.
+template <int ORDER, typename R>
+__device__ __forceinline__ void gather6(const FieldView<R>* F, int ci, int cj, int ck, R ox,
+                                        R oy, R oz, R* eb) {
+  NodeCO<ORDER, R> nx, ny, nz;
+  StagCO<ORDER, R> sx, sy, sz;
+  nx.set(ox); ny.set(oy); nz.set(oz);
+  sx.set(ox); sy.set(oy); sz.set(oz);
+  constexpr int N = ORDER + 1, S = ORDER;
+  eb[0] = gsum<S, N, N>(F[0], ci + sx.r0, sx.s, cj + ny.r0, ny.s, ck + nz.r0, nz.s);
+  eb[1] = gsum<N, S, N>(F[1], ci + nx.r0, nx.s, cj + sy.r0, sy.s, ck + nz.r0, nz.s);
+  eb[2] = gsum<N, N, S>(F[2], ci + nx.r0, nx.s, cj + ny.r0, ny.s, ck + sz.r0, sz.s);
+  eb[3] = gsum<N, S, S>(F[3], ci + nx.r0, nx.s, cj + sy.r0, sy.s, ck + sz.r0, sz.s);
+  eb[4] = gsum<S, N, S>(F[4], ci + sx.r0, sx.s, cj + ny.r0, ny.s, ck + sz.r0, sz.s);
+  eb[5] = gsum<S, S, N>(F[5], ci + sx.r0, sx.s, cj + sy.r0, sy.s, ck + nz.r0, nz.s);
+}
+
+// Accumulator target for the deposition: shared window (atomicAdd on A) or
+// the global periodic FP64 grid.
+template <typename A> struct SmemAcc {
+  A* p;
+  int sy, sz;
+  __device__ __forceinline__ void add(int i, int j, int k, A v) const {
+    atomicAdd(p + i + sy * j + sz * k, v);
+  }
+};
+struct GlobAcc {
+  double* p;
+  int nx, ny, nz;
+  __device__ __forceinline__ static int wrap(int i, int n) {
+    return i < 0 ? i + n : (i >= n ? i - n : i);
+  }
+  __device__ __forceinline__ void add(int i, int j, int k, double v) const {
+    i = wrap(i, nx); j = wrap(j, ny); k = wrap(k, nz);
+    atomicAdd(p + i + (i64)nx * (j + (i64)ny * k), v);
+  }
+};
+
+// Esirkepov current of one particle into three accumulators, box in the
+// accumulator's coordinates.  Same arithmetic as esirkepov_3d.F90 (prefix
+// sums of W along x for Jx, y for Jy, z for Jz).
+template <int ORDER, typename R, typename ACC, typename AV>
+__device__ __forceinline__ void esirkepov_dep(const EsirAxis<ORDER, R>& X,
+                                              const EsirAxis<ORDER, R>& Y,
+                                              const EsirAxis<ORDER, R>& Z, R wqx, R wqy, R wqz,
+                                              const ACC& jx, const ACC& jy, const ACC& jz) {
+  constexpr int M = ORDER + 2;
+  const R onethird = (R)(1.0 / 3.0);
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    if (k >= Z.n) continue;
+    R dsz = Z.s1[k] - Z.s0[k];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      if (j >= Y.n) continue;
+      R dsy = Y.s1[j] - Y.s0[j];
+      R fyz = (Y.s0[j] + (R)0.5 * dsy) * Z.s0[k] + ((R)0.5 * Y.s0[j] + onethird * dsy) * dsz;
+      R acc = (R)0;
+#pragma unroll
+      for (int i = 0; i < M - 1; ++i) {
+        if (i >= X.n - 1) continue;
+        acc = acc + wqx * (X.s1[i] - X.s0[i]) * fyz;
+        jx.add(X.i0 + i, Y.i0 + j, Z.i0 + k, (AV)acc);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    if (k >= Z.n) continue;
+    R dsz = Z.s1[k] - Z.s0[k];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      if (i >= X.n) continue;
+      R dsx = X.s1[i] - X.s0[i];
+      R fzx = (Z.s0[k] + (R)0.5 * dsz) * X.s0[i] + ((R)0.5 * Z.s0[k] + onethird * dsz) * dsx;
+      R acc = (R)0;
+#pragma unroll
+      for (int j = 0; j < M - 1; ++j) {
+        if (j >= Y.n - 1) continue;
+        acc = acc + wqy * (Y.s1[j] - Y.s0[j]) * fzx;
+        jy.add(X.i0 + i, Y.i0 + j, Z.i0 + k, (AV)acc);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    if (j >= Y.n) continue;
+    R dsy = Y.s1[j] - Y.s0[j];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      if (i >= X.n) continue;
+      R dsx = X.s1[i] - X.s0[i];
+      R fxy = (X.s0[i] + (R)0.5 * dsx) * Y.s0[j] + ((R)0.5 * X.s0[i] + onethird * dsx) * dsy;
+      R acc = (R)0;
+#pragma unroll
+      for (int k = 0; k < M - 1; ++k) {
+        if (k >= Z.n - 1) continue;
+        acc = acc + wqz * (Z.s1[k] - Z.s0[k]) * fxy;
+        jz.add(X.i0 + i, Y.i0 + j, Z.i0 + k, (AV)acc);
+      }
+    }
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void cell_step(R& o, int& c, R du) {
+  // o + du, split into cell shift and offset in [0,1)
+  R on = o + du;
+  R fl = floor(on);
+  int s = (int)fl;
+  R of = on - fl;
+  if (of >= (R)1) { of = of - (R)1; s += 1; }
+  o = of;
+  c += s;
+}
+
+template <typename R> __device__ __forceinline__ R rsqrt_(R x);
+template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return 1.0f / sqrtf(x); }
+template <> __device__ __forceinline__ double rsqrt_<double>(double x) { return 1.0 / sqrt(x); }
+
+// Shared-memory current accumulators (MODE):
+//  0  FP32 atomics;
+//  1  int32 fixed point, one word (scale 2^29 / node bound);
+//  2  64-bit fixed point as two native int32 words: the value X (an integer,
+//     |X| <= 2^42 per node by the scale) is split X = hi*2^12 + lo with
+//     lo in [0, 2^12); both words are summed with int32 atomics and the sums
+//     cannot overflow (|sum hi| <= 2^30, sum lo < 2^32 for < 2^20 terms);
+//  3  FP64 atomics (FP64 engine).
+// Fixed-point sums are order-independent, so a tile's current does not
+// depend on the atomics' ordering.
+template <int MODE> struct Acc;
+template <> struct Acc<0> {
+  typedef float T;
+  static constexpr int NW = 1;
+  static constexpr double SCALE_BITS = 0.0;
+  __device__ __forceinline__ static void add(float* p, float v, int) { atomicAdd(p, v); }
+  __device__ __forceinline__ static double get(const float* p, int r, int) { return p[r]; }
+};
+template <> struct Acc<1> {
+  typedef int T;
+  static constexpr int NW = 1;
+  static constexpr double SCALE_BITS = 536870912.0;   // 2^29
+  __device__ __forceinline__ static void add(int* p, float v, int) { atomicAdd(p, __float2int_rn(v)); }
+  __device__ __forceinline__ static double get(const int* p, int r, int) { return (double)p[r]; }
+};
+template <> struct Acc<2> {
+  typedef int T;
+  static constexpr int NW = 2;
+  static constexpr double SCALE_BITS = 4398046511104.0;  // 2^42
+  __device__ __forceinline__ static void add(int* p, float v, int V3) {
+    const long long X = __float2ll_rn(v);
+    atomicAdd(p, (int)(X >> 12));
+    atomicAdd(reinterpret_cast<unsigned*>(p + V3), (unsigned)(X & 0xFFF));
+  }
+  __device__ __forceinline__ static double get(const int* p, int r, int V3) {
+    return (double)p[r] * 4096.0 + (double)reinterpret_cast<const unsigned*>(p)[r + V3];
+  }
+};
+template <> struct Acc<3> {
+  typedef double T;
+  static constexpr int NW = 1;
+  static constexpr double SCALE_BITS = 0.0;
+  __device__ __forceinline__ static void add(double* p, double v, int) { atomicAdd(p, v); }
+  __device__ __forceinline__ static double get(const double* p, int r, int) { return p[r]; }
+};
+
+// Esirkepov deposit in outer-product form: for Jx,
+//   J(i,j,k) += cx * C_x(i) * F_yz(j,k),  C_x(i) = sum_{i'<=i} (s1 - s0)_x(i'),
+//   F_yz = (s0y + ds_y/2) s0z + (s0y/2 + ds_y/3) ds_z,
+// which is the reference's prefix sum of W_x (esirkepov_3d.F90:198-233) with
+// the common factor taken out.  Box offsets are compile-time; the boxes'
+// origins are runtime.  Window variant: shared memory, strides SY, SZ.
+template <int ORDER, typename R, int MODE, int SY, int SZ, int V>
+__device__ __forceinline__ void dep_window(typename Acc<MODE>::T* Js, const EsirAxis<ORDER, R>& X,
+                                           const EsirAxis<ORDER, R>& Y,
+                                           const EsirAxis<ORDER, R>& Z, R cx, R cy, R cz) {
+  constexpr int M = ORDER + 2;
+  const R third = (R)(1.0 / 3.0);
+  typename Acc<MODE>::T* bx = Js + X.i0 + Y.i0 * SY + Z.i0 * SZ;
+  typename Acc<MODE>::T* by = bx + V;
+  typename Acc<MODE>::T* bz = bx + 2 * V;
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    if (k >= Z.n) continue;
+    const R s0z = Z.s0[k], dsz = Z.s1[k] - s0z;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      if (j >= Y.n) continue;
+      const R s0y = Y.s0[j], dsy = Y.s1[j] - s0y;
+      const R f = ((s0y + (R)0.5 * dsy) * s0z + ((R)0.5 * s0y + third * dsy) * dsz) * cx;
+      R C = (R)0;
+#pragma unroll
+      for (int i = 0; i < M - 1; ++i) {
+        if (i >= X.n - 1) continue;
+        C += X.s1[i] - X.s0[i];
+        Acc<MODE>::add(bx + i + j * SY + k * SZ, C * f, 3 * V);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    if (k >= Z.n) continue;
+    const R s0z = Z.s0[k], dsz = Z.s1[k] - s0z;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      if (i >= X.n) continue;
+      const R s0x = X.s0[i], dsx = X.s1[i] - s0x;
+      const R f = ((s0z + (R)0.5 * dsz) * s0x + ((R)0.5 * s0z + third * dsz) * dsx) * cy;
+      R C = (R)0;
+#pragma unroll
+      for (int j = 0; j < M - 1; ++j) {
+        if (j >= Y.n - 1) continue;
+        C += Y.s1[j] - Y.s0[j];
+        Acc<MODE>::add(by + i + j * SY + k * SZ, C * f, 3 * V);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    if (j >= Y.n) continue;
+    const R s0y = Y.s0[j], dsy = Y.s1[j] - s0y;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      if (i >= X.n) continue;
+      const R s0x = X.s0[i], dsx = X.s1[i] - s0x;
+      const R f = ((s0x + (R)0.5 * dsx) * s0y + ((R)0.5 * s0x + third * dsx) * dsy) * cz;
+      R C = (R)0;
+#pragma unroll
+      for (int k = 0; k < M - 1; ++k) {
+        if (k >= Z.n - 1) continue;
+        C += Z.s1[k] - Z.s0[k];
+        Acc<MODE>::add(bz + i + j * SY + k * SZ, C * f, 3 * V);
+      }
+    }
+  }
+}
+
+// Fast path of the window deposit: no node change along any axis (the common
+// case), box of ORDER+1 nodes per axis starting at `base`; t0 = shape at the
+// new position, t1 = shape at the old position on the same nodes.
+template <int ORDER, typename R, int MODE, int SY, int SZ, int V>
+__device__ __forceinline__ void dep_window_same(typename Acc<MODE>::T* base, const R* t0x,
+                                                const R* t1x, const R* t0y, const R* t1y,
+                                                const R* t0z, const R* t1z, R cx, R cy, R cz) {
+  constexpr int N = ORDER + 1;
+  const R third = (R)(1.0 / 3.0);
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const R s0z = t0z[k], dsz = t1z[k] - s0z;
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      const R s0y = t0y[j], dsy = t1y[j] - s0y;
+      const R f = ((s0y + (R)0.5 * dsy) * s0z + ((R)0.5 * s0y + third * dsy) * dsz) * cx;
+      R C = (R)0;
+#pragma unroll
+      for (int i = 0; i < N - 1; ++i) {
+        C += t1x[i] - t0x[i];
+        Acc<MODE>::add(base + i + j * SY + k * SZ, C * f, 3 * V);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const R s0z = t0z[k], dsz = t1z[k] - s0z;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const R s0x = t0x[i], dsx = t1x[i] - s0x;
+      const R f = ((s0z + (R)0.5 * dsz) * s0x + ((R)0.5 * s0z + third * dsz) * dsx) * cy;
+      R C = (R)0;
+#pragma unroll
+      for (int j = 0; j < N - 1; ++j) {
+        C += t1y[j] - t0y[j];
+        Acc<MODE>::add(base + V + i + j * SY + k * SZ, C * f, 3 * V);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const R s0y = t0y[j], dsy = t1y[j] - s0y;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const R s0x = t0x[i], dsx = t1x[i] - s0x;
+      const R f = ((s0x + (R)0.5 * dsx) * s0y + ((R)0.5 * s0x + third * dsx) * dsy) * cz;
+      R C = (R)0;
+#pragma unroll
+      for (int k = 0; k < N - 1; ++k) {
+        C += t1z[k] - t0z[k];
+        Acc<MODE>::add(base + 2 * V + i + j * SY + k * SZ, C * f, 3 * V);
+      }
+    }
+  }
+}
+
+// General window deposit (a node changes along some axis), kept out of line.
+template <int ORDER, typename R, int MODE, int SY, int SZ, int V>
+__device__ __noinline__ void dep_window_general(typename Acc<MODE>::T* Js,
+                                                const EsirAxis<ORDER, R>& X,
+                                                const EsirAxis<ORDER, R>& Y,
+                                                const EsirAxis<ORDER, R>& Z, R cx, R cy, R cz) {
+  dep_window<ORDER, R, MODE, SY, SZ, V>(Js, X, Y, Z, cx, cy, cz);
+}
+
+// Global variant (particles outside their tile window): FP64 atomics on the
+// periodic J grid, in the reference's W-prefix form (unscaled coefficients).
+template <int ORDER, typename R>
+__device__ __noinline__ void dep_global(const Job& J, const EsirAxis<ORDER, R>& X,
+                                        const EsirAxis<ORDER, R>& Y,
+                                        const EsirAxis<ORDER, R>& Z, R cx, R cy, R cz) {
+  GlobAcc G[3];
+  G[0].p = J.jx; G[1].p = J.jy; G[2].p = J.jz;
+  for (int c = 0; c < 3; ++c) { G[c].nx = J.nx; G[c].ny = J.ny; G[c].nz = J.nz; }
+  esirkepov_dep<ORDER, R, GlobAcc, double>(X, Y, Z, cx, cy, cz, G[0], G[1], G[2]);
+}
+
+template <int ORDER, typename R>
+__device__ __noinline__ void gather_global(const Job& J, int ci, int cj, int ck, R ox, R oy,
+                                           R oz, R* eb) {
+  const int G = J.g, pitch = J.pitch_x, NYg = J.pitch_y;
+  FieldView<R> F[6];
+  const void* src[6] = {J.ex, J.ey, J.ez, J.bx, J.by, J.bz};
+  for (int c = 0; c < 6; ++c) {
+    F[c].p = (const R*)src[c] + (G + (i64)pitch * (G + (i64)NYg * G));
+    F[c].sy = pitch; F[c].sz = pitch * NYg;
+  }
+  gather6<ORDER, R>(F, ci, cj, ck, ox, oy, oz, eb);
+}
+
+// Gather from the shared window with compile-time strides: each component's
+// support starts at `base`, points at base + t + b*SY + c*SZ.
+template <int NA, int NB, int NC, int SY, int SZ, typename R>
+__device__ __forceinline__ R gwin(const R* base, const R* sa, const R* sb, const R* sc) {
+  R out = (R)0;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    R a = (R)0;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      R r = (R)0;
+#pragma unroll
+      for (int t = 0; t < NA; ++t) r = r + sa[t] * base[t + b * SY + c * SZ];
+      a = a + r * sb[b];
+    }
+    out = out + a * sc[c];
+  }
+  return out;
+}
+
+constexpr int MAX_THREADS = 256;
+// Per-tile queue of window particles whose node changes along some axis: they
+// are deposited after the tile's main loop by full warps, so the common
+// same-node path never diverges into the general one.
+constexpr int QCAP = 256;
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// The fused particle kernel.  Persistent CTAs pull (job, tile) work items;
+// tile edge T (cells), window margin D: compile-time, so every shared-memory
+// address of the gather and of the deposition is a register plus an
+// immediate.  Windows of partial tiles extend into the padded guard region of
+// the field arrays (never written, zero) which no particle reaches.
+// ---------------------------------------------------------------------------
+template <typename R, int ORDER, int T, int D, int MODE>
+__global__ void __launch_bounds__(MAX_THREADS, 2)
+    k_tile_step(const Job* __restrict__ jobs, const int2* __restrict__ work, int nwork,
+                const int* __restrict__ nwork_dev, int* ctr) {
+  constexpr int L = Reach<ORDER>::L, H = Reach<ORDER>::H;
+  constexpr int W = T + 2 * D + L + H, SY = W, SZ = W * W, V = W * W * W;
+  typedef typename Acc<MODE>::T A;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* Fs = reinterpret_cast<R*>(smem_raw);
+  A* Js = reinterpret_cast<A*>(smem_raw + (size_t)6 * V * sizeof(R));
+  unsigned char* qbase = smem_raw + (size_t)6 * V * sizeof(R) + (size_t)3 * V * Acc<MODE>::NW * sizeof(A);
+  R* q_o = reinterpret_cast<R*>(qbase);                                 // [3][QCAP]
+  int* q_ip = reinterpret_cast<int*>(qbase + 3 * QCAP * sizeof(R));      // [QCAP]
+  unsigned* q_pk = reinterpret_cast<unsigned*>(q_ip + QCAP);             // [QCAP]
+  __shared__ Job sj;
+  __shared__ int s_item;
+  __shared__ int s_qn;
+  __shared__ float s_max[5][MAX_THREADS / 32];
+  __shared__ double s_red[MAX_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+
+  if (nwork_dev) nwork = min(nwork, *nwork_dev);
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_item = atomicAdd(ctr, 1);
+      s_qn = 0;
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nwork) break;
+    const int2 wk = work[item];
+    {
+      const int nw = (int)(sizeof(Job) / sizeof(int));
+      const int* src = reinterpret_cast<const int*>(jobs + wk.x);
+      int* dst = reinterpret_cast<int*>(&sj);
+      for (int t = threadIdx.x; t < nw; t += blockDim.x) dst[t] = src[t];
+    }
+    __syncthreads();
+    const int nx = sj.nx, ny = sj.ny, nz = sj.nz, G = sj.g;
+    const int tile = wk.y;
+    const int ti = tile % sj.ntx, tj = (tile / sj.ntx) % sj.nty, tk = tile / (sj.ntx * sj.nty);
+    const int c0x = ti * T, c0y = tj * T, c0z = tk * T;
+    const int tex = min(T, nx - c0x), tey = min(T, ny - c0y), tez = min(T, nz - c0z);
+    const int wox = c0x - D - L, woy = c0y - D - L, woz = c0z - D - L;
+    const int pbeg = sj.tile_off[tile], pend = sj.tile_off[tile + 1];
+    // ---- stage the E/B window; track |E|, |B| maxima -----------------------
+    const int pitch = sj.pitch_x, NYg = sj.pitch_y;
+    float emax = 0.f, bmax = 0.f;
+    {
+      const i64 base0 = (i64)(wox + G) + (i64)pitch * ((woy + G) + (i64)NYg * (woz + G));
+#pragma unroll 1
+      for (int comp = 0; comp < 6; ++comp) {
+        const R* src = (const R*)(comp == 0 ? sj.ex : comp == 1 ? sj.ey : comp == 2 ? sj.ez
+                                 : comp == 3 ? sj.bx : comp == 4 ? sj.by : sj.bz) + base0;
+        R* dst = Fs + comp * V;
+        float m = 0.f;
+        for (int r = threadIdx.x; r < V; r += blockDim.x) {
+          const int a = r % W, b = (r / W) % W, c = r / SZ;
+          const R v = __ldg(src + a + (i64)pitch * (b + (i64)NYg * c));
+          dst[r] = v;
+          m = fmaxf(m, fabsf((float)v));
+        }
+        if (comp < 3) emax = fmaxf(emax, m); else bmax = fmaxf(bmax, m);
+      }
+    }
+    for (int e = threadIdx.x; e < 3 * V * Acc<MODE>::NW; e += blockDim.x) Js[e] = (A)0;
+    // ---- fixed-point scale of the current window (FP32 engine) -------------
+    // Bound of one particle's contribution to one node of J_c:
+    //   |q| w_max / (dt dV / d_c) * (max displacement along c in cells),
+    // with the displacement bounded from max |u| of the tile's particles
+    // before the push plus the push's change |q| dt / m (|E| + c |B|).
+    // A node of the window receives deposits only from particles whose old
+    // cell lies within L+H+3 cells of it along every axis, so the node sum
+    // is bounded by (max particles per window cell) * (L+H+3)^3 contributions.
+    float umax2 = 0.f, wmax = 0.f, cmax = 0.f;
+    constexpr bool FIXED = MODE == 1 || MODE == 2;
+    if (FIXED) {
+      int* hist = reinterpret_cast<int*>(Js) + 2 * V;   // zero; re-zeroed below
+      __syncthreads();
+      const R* uxp = (const R*)sj.ux; const R* uyp = (const R*)sj.uy;
+      const R* uzp = (const R*)sj.uz; const R* wp = (const R*)sj.w;
+      for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
+        float a = (float)uxp[ip], b = (float)uyp[ip], c = (float)uzp[ip];
+        umax2 = fmaxf(umax2, a * a + b * b + c * c);
+        wmax = fmaxf(wmax, fabsf((float)wp[ip]));
+        int ci, cj, ck;
+        unpack_cell(sj.cell[ip], ci, cj, ck);
+        int vx = ci - c0x, vy = cj - c0y, vz = ck - c0z;
+        if (vx > tex - 1 + D) vx -= nx; else if (vx < -D) vx += nx;
+        if (vy > tey - 1 + D) vy -= ny; else if (vy < -D) vy += ny;
+        if (vz > tez - 1 + D) vz -= nz; else if (vz < -D) vz += nz;
+        if (vx >= -D && vx <= tex - 1 + D && vy >= -D && vy <= tey - 1 + D && vz >= -D &&
+            vz <= tez - 1 + D)
+          atomicAdd(hist + (vx + D + L) + (vy + D + L) * SY + (vz + D + L) * SZ, 1);
+      }
+      __syncthreads();
+      for (int r = threadIdx.x; r < V; r += blockDim.x) {
+        cmax = fmaxf(cmax, (float)hist[r]);
+        hist[r] = 0;
+      }
+    }
+    emax = warp_max(emax); bmax = warp_max(bmax); umax2 = warp_max(umax2); wmax = warp_max(wmax);
+    cmax = warp_max(cmax);
+    if (lane == 0) {
+      s_max[0][wid] = emax; s_max[1][wid] = bmax; s_max[2][wid] = umax2; s_max[3][wid] = wmax;
+      s_max[4][wid] = cmax;
+    }
+    __syncthreads();
+    double scale[3];
+    scale[0] = scale[1] = scale[2] = 1.0;
+    if (FIXED) {
+      float E = 0.f, B = 0.f, U2 = 0.f, Wm = 0.f, Cm = 0.f;
+      for (int w = 0; w < nwarps; ++w) {
+        E = fmaxf(E, s_max[0][w]); B = fmaxf(B, s_max[1][w]);
+        U2 = fmaxf(U2, s_max[2][w]); Wm = fmaxf(Wm, s_max[3][w]); Cm = fmaxf(Cm, s_max[4][w]);
+      }
+      const double c = sj.clight;
+      const double ub = sqrt((double)U2) +
+                        fabs(sj.q) / sj.m * sj.dt * (1.7320508075688772 * ((double)E + c * B));
+      const double vb = ub / sqrt(1.0 + ub * ub / (c * c));
+      const double dV = sj.dx * sj.dy * sj.dz;
+      constexpr int reach = L + H + 3;
+      const double np_ = fmax((double)Cm * (reach * reach * reach), 1.0);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double dq = q == 0 ? sj.dx : (q == 1 ? sj.dy : sj.dz);
+        const double disp = fmin(vb * sj.dt / dq, 1.0);
+        const double bound = fabs(sj.q) * (double)Wm * dq / (sj.dt * dV) * disp;
+        const double s = Acc<MODE>::SCALE_BITS / fmax(np_ * bound, 1e-300);
+        scale[q] = fmin(s, 1e30);
+      }
+    }
+    // ---- particles -----------------------------------------------------------
+    const R dtdx = (R)(sj.dt / sj.dx), dtdy = (R)(sj.dt / sj.dy), dtdz = (R)(sj.dt / sj.dz);
+    const R clghtisq = (R)(1.0 / (sj.clight * sj.clight));
+    const R cst_b = (R)(sj.q * sj.dt * 0.5 / sj.m), cst_v = (R)(sj.q * sj.dt / sj.m);
+    const R invc = (R)(1.0 / sj.clight);
+    const double c2i = 1.0 / (sj.clight * sj.clight);
+    const R qdx = (R)(sj.q / (sj.dt * sj.dy * sj.dz)), qdy = (R)(sj.q / (sj.dt * sj.dx * sj.dz)),
+            qdz = (R)(sj.q / (sj.dt * sj.dx * sj.dy));
+    const R scx = (R)scale[0], scy = (R)scale[1], scz = (R)scale[2];
+    const bool vay = sj.pusher == 1;
+    uint32_t* cellp = sj.cell;
+    R *oxp = (R*)sj.ox, *oyp = (R*)sj.oy, *ozp = (R*)sj.oz;
+    R *uxp = (R*)sj.ux, *uyp = (R*)sj.uy, *uzp = (R*)sj.uz;
+    const R* wp = (const R*)sj.w;
+    double ke = 0.0;
+    int nslow = 0, bad = 0;
+    __syncthreads();
+
+    for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
+      int ci, cj, ck;
+      unpack_cell(cellp[ip], ci, cj, ck);
+      const R ox = oxp[ip], oy = oyp[ip], oz = ozp[ip];
+      R ux = uxp[ip], uy = uyp[ip], uz = uzp[ip];
+      const R wgt = wp[ip];
+      int vx = ci - c0x, vy = cj - c0y, vz = ck - c0z;
+      if (vx > tex - 1 + D) vx -= nx; else if (vx < -D) vx += nx;
+      if (vy > tey - 1 + D) vy -= ny; else if (vy < -D) vy += ny;
+      if (vz > tez - 1 + D) vz -= nz; else if (vz < -D) vz += nz;
+      const bool in_old = vx >= -D && vx <= tex - 1 + D && vy >= -D && vy <= tey - 1 + D &&
+                          vz >= -D && vz <= tez - 1 + D;
+      // ---- gather ----------------------------------------------------------
+      R eb[6];
+      if (in_old) {
+        const int wx = vx + D + L, wy = vy + D + L, wz = vz + D + L;
+        NodeCO<ORDER, R> nxs, nys, nzs;
+        StagCO<ORDER, R> sxs, sys, szs;
+        nxs.set(ox); nys.set(oy); nzs.set(oz);
+        sxs.set(ox); sys.set(oy); szs.set(oz);
+        constexpr int N = ORDER + 1, S = ORDER;
+        const R* F0 = Fs + wx + wy * SY + wz * SZ;
+        eb[0] = gwin<S, N, N, SY, SZ>(F0 + sxs.r0 + nys.r0 * SY + nzs.r0 * SZ, sxs.s, nys.s, nzs.s);
+        eb[1] = gwin<N, S, N, SY, SZ>(F0 + V + nxs.r0 + sys.r0 * SY + nzs.r0 * SZ, nxs.s, sys.s, nzs.s);
+        eb[2] = gwin<N, N, S, SY, SZ>(F0 + 2 * V + nxs.r0 + nys.r0 * SY + szs.r0 * SZ, nxs.s, nys.s, szs.s);
+        eb[3] = gwin<N, S, S, SY, SZ>(F0 + 3 * V + nxs.r0 + sys.r0 * SY + szs.r0 * SZ, nxs.s, sys.s, szs.s);
+        eb[4] = gwin<S, N, S, SY, SZ>(F0 + 4 * V + sxs.r0 + nys.r0 * SY + szs.r0 * SZ, sxs.s, nys.s, szs.s);
+        eb[5] = gwin<S, S, N, SY, SZ>(F0 + 5 * V + sxs.r0 + sys.r0 * SY + nzs.r0 * SZ, sxs.s, sys.s, nzs.s);
+      } else {
+        gather_global<ORDER, R>(sj, ci, cj, ck, ox, oy, oz, eb);
+      }
+      // ---- push ------------------------------------------------------------
+      R gi;
+      if (vay) {
+        gi = rsqrt_<R>((R)1 + (ux * ux + uy * uy + uz * uz) * clghtisq);
+        vay_push(ux, uy, uz, gi, eb[0], eb[1], eb[2], eb[3], eb[4], eb[5], cst_v, invc, clghtisq);
+      } else {
+        boris_push(ux, uy, uz, gi, eb[0], eb[1], eb[2], eb[3], eb[4], eb[5], cst_b, clghtisq);
+        set_gamma(ux, uy, uz, gi, clghtisq);
+      }
+      // ---- position: exact old (c, o) -> new (c + s, o') ----------------------
+      R nox = ox, noy = oy, noz = oz;
+      int sx = 0, sy = 0, sz = 0;
+      cell_step(nox, sx, ux * gi * dtdx);
+      cell_step(noy, sy, uy * gi * dtdy);
+      cell_step(noz, sz, uz * gi * dtdz);
+      const bool in_new = in_old && vx + sx >= -D && vx + sx <= tex - 1 + D &&
+                          vy + sy >= -D && vy + sy <= tey - 1 + D && vz + sz >= -D &&
+                          vz + sz <= tez - 1 + D;
+      // ---- deposition --------------------------------------------------------
+      {
+        int r0x, r1x, r0y, r1y, r0z, r1z;
+        R x0, x1, y0, y1, z0, z1;
+        esir_node<ORDER, R>(nox, r0x, x0); esir_node<ORDER, R>(ox, r1x, x1);
+        esir_node<ORDER, R>(noy, r0y, y0); esir_node<ORDER, R>(oy, r1y, y1);
+        esir_node<ORDER, R>(noz, r0z, z0); esir_node<ORDER, R>(oz, r1z, z1);
+        // node indices relative to the old cell: new = shift + r0, old = r1
+        const bool same = (sx + r0x == r1x) && (sy + r0y == r1y) && (sz + r0z == r1z);
+        const R wq = wgt;
+        if (in_new && same) {
+          constexpr int a = ORDER / 2;
+          R t0x[ORDER + 1], t1x[ORDER + 1], t0y[ORDER + 1], t1y[ORDER + 1], t0z[ORDER + 1],
+              t1z[ORDER + 1];
+          EsirAxis<ORDER, R>::shape(x0, t0x); EsirAxis<ORDER, R>::shape(x1, t1x);
+          EsirAxis<ORDER, R>::shape(y0, t0y); EsirAxis<ORDER, R>::shape(y1, t1y);
+          EsirAxis<ORDER, R>::shape(z0, t0z); EsirAxis<ORDER, R>::shape(z1, t1z);
+          A* base = Js + (vx + D + L + r1x - a) + (vy + D + L + r1y - a) * SY +
+                    (vz + D + L + r1z - a) * SZ;
+          dep_window_same<ORDER, R, MODE, SY, SZ, V>(base, t0x, t1x, t0y, t1y, t0z, t1z,
+                                                     wq * qdx * scx, wq * qdy * scy,
+                                                     wq * qdz * scz);
+        } else {
+          const int bx = in_new ? vx + D + L : ci;
+          const int by = in_new ? vy + D + L : cj;
+          const int bz = in_new ? vz + D + L : ck;
+          EsirAxis<ORDER, R> EX, EY, EZ;
+          bool ok = EX.set(bx + sx + r0x, x0, bx + r1x, x1);
+          ok = EY.set(by + sy + r0y, y0, by + r1y, y1) && ok;
+          ok = EZ.set(bz + sz + r0z, z0, bz + r1z, z1) && ok;
+          if (!ok) bad = 1;
+          if (in_new) {
+            const int q = atomicAdd(&s_qn, 1);
+            if (q < QCAP) {
+              q_ip[q] = ip;
+              q_pk[q] = (unsigned)(vx + D + L) | ((unsigned)(vy + D + L) << 8) |
+                        ((unsigned)(vz + D + L) << 16) | ((unsigned)(sx + 1) << 24) |
+                        ((unsigned)(sy + 1) << 26) | ((unsigned)(sz + 1) << 28);
+              q_o[q] = ox; q_o[QCAP + q] = oy; q_o[2 * QCAP + q] = oz;
+            } else {
+              dep_window_general<ORDER, R, MODE, SY, SZ, V>(Js, EX, EY, EZ, wq * qdx * scx,
+                                                            wq * qdy * scy, wq * qdz * scz);
+            }
+          } else {
+            ++nslow;
+            dep_global<ORDER, R>(sj, EX, EY, EZ, wq * qdx, wq * qdy, wq * qdz);
+          }
+        }
+      }
+      // ---- store -------------------------------------------------------------
+      int nci = ci + sx, ncj = cj + sy, nck = ck + sz;
+      nci = nci < 0 ? nci + nx : (nci >= nx ? nci - nx : nci);
+      ncj = ncj < 0 ? ncj + ny : (ncj >= ny ? ncj - ny : ncj);
+      nck = nck < 0 ? nck + nz : (nck >= nz ? nck - nz : nck);
+      cellp[ip] = pack_cell(nci, ncj, nck);
+      oxp[ip] = nox; oyp[ip] = noy; ozp[ip] = noz;
+      uxp[ip] = ux; uyp[ip] = uy; uzp[ip] = uz;
+      const double u2 = (double)ux * ux + (double)uy * uy + (double)uz * uz;
+      ke += u2 * c2i / (1.0 + sqrt(1.0 + u2 * c2i)) * (double)wgt;
+    }
+    __syncthreads();
+    // ---- deferred window particles with a node change ------------------------
+    {
+      const int nq = min(s_qn, QCAP);
+      for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const int ip = q_ip[q];
+        const unsigned pk = q_pk[q];
+        const int bx = pk & 255u, by = (pk >> 8) & 255u, bz = (pk >> 16) & 255u;
+        const int sx = (int)((pk >> 24) & 3u) - 1, sy = (int)((pk >> 26) & 3u) - 1,
+                  sz = (int)((pk >> 28) & 3u) - 1;
+        const R ox = q_o[q], oy = q_o[QCAP + q], oz = q_o[2 * QCAP + q];
+        const R nox = oxp[ip], noy = oyp[ip], noz = ozp[ip], wq = wp[ip];
+        int r0, r1;
+        R a0, a1;
+        EsirAxis<ORDER, R> EX, EY, EZ;
+        esir_node<ORDER, R>(nox, r0, a0); esir_node<ORDER, R>(ox, r1, a1);
+        bool ok = EX.set(bx + sx + r0, a0, bx + r1, a1);
+        esir_node<ORDER, R>(noy, r0, a0); esir_node<ORDER, R>(oy, r1, a1);
+        ok = EY.set(by + sy + r0, a0, by + r1, a1) && ok;
+        esir_node<ORDER, R>(noz, r0, a0); esir_node<ORDER, R>(oz, r1, a1);
+        ok = EZ.set(bz + sz + r0, a0, bz + r1, a1) && ok;
+        if (!ok) bad = 1;
+        dep_window<ORDER, R, MODE, SY, SZ, V>(Js, EX, EY, EZ, wq * qdx * scx, wq * qdy * scy,
+                                              wq * qdz * scz);
+      }
+    }
+    __syncthreads();
+    // ---- flush the J window: FP64 atomics into the periodic grid -------------
+    {
+#pragma unroll 1
+      for (int comp = 0; comp < 3; ++comp) {
+        double* dst = comp == 0 ? sj.jx : comp == 1 ? sj.jy : sj.jz;
+        const double inv = 1.0 / (comp == 0 ? scale[0] : comp == 1 ? scale[1] : scale[2]);
+        const A* src = Js + comp * V;
+        for (int r = threadIdx.x; r < V; r += blockDim.x) {
+          const double v = Acc<MODE>::get(src, r, 3 * V);
+          if (v == 0.0) continue;
+          const int a = r % W, b = (r / W) % W, c = r / SZ;
+          const int gi = GlobAcc::wrap(wox + a, nx), gj = GlobAcc::wrap(woy + b, ny),
+                    gk = GlobAcc::wrap(woz + c, nz);
+          atomicAdd(dst + gi + (i64)nx * (gj + (i64)ny * gk), v * inv);
+        }
+      }
+    }
+    // ---- kinetic energy of the tile ------------------------------------------
+    {
+      double v = ke;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0) s_red[wid] = v;
+      if (nslow) atomicAdd(&sj.counters[0], nslow);
+      if (bad) atomicExch(&sj.counters[1], 1);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < nwarps; ++w) t += s_red[w];
+        sj.ke_tile[tile] = t * sj.m * sj.clight * sj.clight;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace pxrt

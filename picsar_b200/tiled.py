@@ -34,19 +34,19 @@ class TiledJob(C.Structure):
     """Mirror of ``pxrb_tiled_job`` (include/picsar_b200.h)."""
     _fields_ = (
         [(n, C.c_int32) for n in ("nx", "ny", "nz", "tx", "ty", "tz", "ntx", "nty", "ntz", "g",
-                                  "pitch_x", "order", "pusher", "drift", "prec", "pad0")]
+                                  "pitch_x", "order", "pusher", "drift", "prec", "pitch_y")]
         + [("np", C.c_int64)]
         + [(n, C.c_double) for n in ("dx", "dy", "dz", "dt", "q", "m", "clight", "mu0", "eps0",
                                      "xmin", "ymin", "zmin")]
         + [(n, _P) for n in ("ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz", "cell", "ox",
                              "oy", "oz", "ux", "uy", "uz", "w", "cell_b", "ox_b", "oy_b", "oz_b",
                              "ux_b", "uy_b", "uz_b", "w_b", "pid", "pid_b", "tile_off",
-                             "tile_cnt", "ke_tile", "counters")]
+                             "tile_cnt", "ke_tile", "counters", "cell_cnt", "rank_b")]
     )
 
 
 _lib.register({
-    "pxrb_tiled_particle_step": "p I I p I p p I I i s",
+    "pxrb_tiled_particle_step": "p I I I I I p I p p I I i s",
     "pxrb_tiled_push_b": "p I I p i d s",
     "pxrb_tiled_push_e": "p I I p i I s",
     "pxrb_tiled_sort": "p p s",
@@ -55,14 +55,15 @@ _lib.register({
     "pxrb_tiled_field_import": "p I p i s",
     "pxrb_tiled_field_export": "p I p i s",
     "pxrb_tiled_diagnostics": "p p p i p s",
-    "pxrb_tiled_smem_bytes": "=i I I I I I I",
+    "pxrb_tiled_smem_bytes": "=i I I I I I I I",
     "pxrb_tiled_job_size": "=i",
     "pxrb_tiled_diag_scratch": "=i p",
 })
 
 
-def smem_bytes(order, prec, tile, drift):
-    return _lib.query("pxrb_tiled_smem_bytes", order, prec, tile[0], tile[1], tile[2], drift)
+def smem_bytes(order, prec, acc, tile, drift):
+    return _lib.query("pxrb_tiled_smem_bytes", order, prec, acc, tile[0], tile[1], tile[2],
+                      drift)
 
 
 def _check_layout():
@@ -72,6 +73,10 @@ def _check_layout():
 
 
 _I32MAX = 2 ** 31 - 1
+# (tile edge, window margin) pairs the particle kernel is compiled for
+SUPPORTED_SHAPES = {(8, 1), (8, 0), (8, 2), (4, 1), (4, 0)}
+# accumulator modes compiled for the FP32 engine per shape (FP64 engine: mode 3)
+SUPPORTED_ACC = {(8, 1): (0, 1, 2)}
 
 
 @dataclass
@@ -82,6 +87,7 @@ class TiledConfig:
     threads: int = 256
     ctas_per_sm: int = 2
     sort_interval: int = 20
+    acc: int = 2                # FP32 engine current accumulator (see picsar_b200.h)
 
 
 def _stream():
@@ -112,7 +118,10 @@ class TiledSim:
             dt = 0.95 / (clight * math.sqrt(sum(1.0 / v ** 2 for v in self.d)))
         self.dt = float(dt)
         self.q, self.m, self.clight, self.mu0, self.eps0 = q, m, clight, mu0, eps0
-        tile = tuple(int(min(t, v)) for t, v in zip(cfg.tile, self.n))
+        tile = tuple(int(t) for t in cfg.tile)
+        if not (tile[0] == tile[1] == tile[2]) or (tile[0], cfg.drift) not in SUPPORTED_SHAPES:
+            raise ValueError(f"tile {tile} with drift {cfg.drift} not compiled; "
+                             f"supported (edge, drift): {sorted(SUPPORTED_SHAPES)}")
         self.tile = tile
         self.g = max(3, cfg.drift + 2)
         if min(self.n) < 2 * self.g:
@@ -120,8 +129,10 @@ class TiledSim:
         self.nt = tuple(-(-v // t) for v, t in zip(self.n, tile))
         self.ntiles = self.nt[0] * self.nt[1] * self.nt[2]
         al = 4 if self.prec == 0 else 2          # 16-byte rows (TMA-compatible pitch)
-        self.pitch = -(-(nx + 2 * self.g) // al) * al
-        fshape = (nz + 2 * self.g, ny + 2 * self.g, self.pitch)
+        # every tile window fits: pad each axis to whole tiles plus guards
+        self.pitch = -(-(self.nt[0] * tile[0] + 2 * self.g) // al) * al
+        self.pitch_y = self.nt[1] * tile[1] + 2 * self.g
+        fshape = (self.nt[2] * tile[2] + 2 * self.g, self.pitch_y, self.pitch)
         dev, rd = self.device, self.rdtype
         self.E = [torch.zeros(fshape, dtype=rd, device=dev) for _ in range(3)]
         self.B = [torch.zeros(fshape, dtype=rd, device=dev) for _ in range(3)]
@@ -130,6 +141,8 @@ class TiledSim:
         self.tile_off = torch.zeros(self.ntiles + 1, dtype=torch.int32, device=dev)
         self.tile_cnt = torch.zeros(self.ntiles + 1, dtype=torch.int32, device=dev)
         self.ke_tile = torch.zeros(self.ntiles, dtype=torch.float64, device=dev)
+        self.cell_cnt = torch.zeros(self.ntiles * tile[0] * tile[1] * tile[2], dtype=torch.int32,
+                                    device=dev)
         self.counters = torch.zeros(4, dtype=torch.int32, device=dev)
         self.work = torch.stack([torch.zeros(self.ntiles, dtype=torch.int32),
                                  torch.arange(self.ntiles, dtype=torch.int32)], 1).contiguous().to(dev)
@@ -142,7 +155,10 @@ class TiledSim:
         self.np = 0
         self.it = 0
         self.launches = 0          # kernels of this library launched so far
-        self.smem = smem_bytes(self.order, self.prec, tile, cfg.drift)
+        self.acc = 3 if self.prec == 1 else cfg.acc
+        if self.prec == 0 and self.acc not in SUPPORTED_ACC.get((tile[0], cfg.drift), (2,)):
+            raise ValueError(f"accumulator mode {self.acc} not compiled for this tile shape")
+        self.smem = smem_bytes(self.order, self.prec, self.acc, tile, cfg.drift)
         props = torch.cuda.get_device_properties(self.device)
         self.num_sms = props.multi_processor_count
         self.job = TiledJob()
@@ -156,6 +172,7 @@ class TiledSim:
         j.tx, j.ty, j.tz = self.tile
         j.ntx, j.nty, j.ntz = self.nt
         j.g, j.pitch_x, j.order, j.pusher = self.g, self.pitch, self.order, self.pusher
+        j.pitch_y = self.pitch_y
         j.drift, j.prec, j.np = self.cfg.drift, self.prec, self.np
         j.dx, j.dy, j.dz = self.d
         j.dt, j.q, j.m, j.clight, j.mu0, j.eps0 = (self.dt, self.q, self.m, self.clight,
@@ -169,6 +186,7 @@ class TiledSim:
             setattr(j, name, t.data_ptr())
         j.tile_off, j.tile_cnt = self.tile_off.data_ptr(), self.tile_cnt.data_ptr()
         j.ke_tile, j.counters = self.ke_tile.data_ptr(), self.counters.data_ptr()
+        j.cell_cnt = self.cell_cnt.data_ptr()
         self._push_job()
 
     def _jp(self):
@@ -199,9 +217,11 @@ class TiledSim:
         self.parts_b = {c: mk() for c in ("ox", "oy", "oz", "ux", "uy", "uz", "w")}
         self.cell = torch.empty(N, dtype=torch.int32, device=dev)
         self.cell_b = torch.empty(N, dtype=torch.int32, device=dev)
+        self.rank_b = torch.empty(N, dtype=torch.int32, device=dev)
         j = self.job
         j.np = N
         j.cell, j.cell_b = self.cell.data_ptr(), self.cell_b.data_ptr()
+        j.rank_b = self.rank_b.data_ptr()
         for c in ("ox", "oy", "oz", "ux", "uy", "uz", "w"):
             setattr(j, c, self.parts[c].data_ptr())
             setattr(j, c + "_b", self.parts_b[c].data_ptr())
@@ -246,7 +266,7 @@ class TiledSim:
     def particle_step(self):
         ctas = min(self.ntiles, self.num_sms * self.cfg.ctas_per_sm)
         _lib.call("pxrb_tiled_particle_step", self.job_dev.data_ptr(), self.order, self.prec,
-                  self.work.data_ptr(), self.ntiles, None, self.ctr.data_ptr(),
+                  self.tile[0], self.cfg.drift, self.acc, self.work.data_ptr(), self.ntiles, None, self.ctr.data_ptr(),
                   self.cfg.threads, ctas, self.smem, _stream())
         self.launches += 1
 

@@ -74,7 +74,7 @@ def test_tiled_fp64_slow_path(cuda, order):
     window and go through the global-memory gather/deposit path."""
     n, g = (16, 16, 16), 3
     st = plasma(n, 2, 0.4, seed=500 + order)
-    o, t = _pair(n, order, 0, "fp64", st, TiledConfig(tile=(4, 8, 8), drift=0, sort_interval=0),
+    o, t = _pair(n, order, 0, "fp64", st, TiledConfig(tile=(4, 4, 4), drift=0, sort_interval=0),
                  random_fields(n, g, seed=7, amp=0.02))
     o.step(3)
     t.step(3, keep_j=True)
@@ -93,6 +93,19 @@ def test_tiled_fp32_one_step(cuda, order, pusher):
     t.step(1, keep_j=True)
     errs = _compare(o, t, g, 2e-5, 1e-6)
     assert errs["jx"] < 2e-5
+
+
+@pytest.mark.parametrize("acc,tol", [(0, 2e-5), (1, 2e-4), (2, 2e-5)])
+def test_tiled_fp32_accumulators(cuda, acc, tol):
+    """The three FP32 current accumulators (FP32 atomics, int32 fixed point,
+    64-bit fixed point in two int32 words) against the FP64 oracle."""
+    n, g = (16, 16, 24), 3
+    st = plasma(n, 8, 0.05, seed=650)
+    fields = random_fields(n, g, seed=750, amp=0.02)
+    o, t = _pair(n, 2, 0, "fp32", st, TiledConfig(tile=(8, 8, 8), acc=acc), fields)
+    o.step(1)
+    t.step(1, keep_j=True)
+    _compare(o, t, g, tol, 1e-6)
 
 
 def _gauss_residual(t, g):
