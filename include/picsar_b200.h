@@ -35,6 +35,7 @@ extern "C" {
 #define PXRB_ELAUNCH 3
 #define PXRB_ESCRATCH 4
 #define PXRB_ERANGE 5
+#define PXRB_ETOOLARGE 6
 
 /* ------------------------------------------------------------------------
  * Plain FP64 path (PICSAR arrays, one thread per particle, FP64 atomics)
@@ -314,6 +315,17 @@ int pxrb_tiled_field_export(const pxrb_tiled_job* job_host, int32_t which, doubl
 int64_t pxrb_tiled_diag_scratch(const pxrb_tiled_job* job_host);
 int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* scratch,
                            int64_t scratch_len, double* out, void* stream);
+
+/* Same diagnostics for callers that cannot allocate device memory (no
+ * counterpart in the reference): the rho grid and the partial sums live in a
+ * static device array owned by the library, so only the job and out (DEVICE
+ * double[9]) are passed; gauss = 0 computes the energies only.  Jobs of more
+ * than 1,048,576 cells are rejected with PXRB_ETOOLARGE.  Every GPU that loads
+ * the library keeps the ~8.1 MiB array until exit; calls share it, so calls
+ * that overlap on the GPU race.  The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress): make it before any stream capture. */
+int pxrb_tiled_diagnostics_noalloc(const pxrb_tiled_job* job_host, int32_t gauss, double* out,
+                                   void* stream);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@
 #include "picsar_b200.h"
 
 #include <cub/block/block_scan.cuh>
+#include <mutex>
 
 namespace pxrt {
 int launch_order1(int, int, int, int, const pxrb_tiled_job*, const int2*, int, const int*, int*, int, int, size_t, cudaStream_t);
@@ -702,3 +703,55 @@ int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Diagnostics without any allocation by the caller.
+//
+// Some callers cannot allocate device memory: a runtime that hands the library
+// only a job descriptor (no allocator of its own), or code that runs inside a
+// memory pool it must not grow.  This variant keeps its scratch -- the rho
+// grid and the per-block partial sums -- in one file-scope device array, so
+// the caller passes nothing but the job and the 9-double output.
+//
+// Limits and rules:
+//  * the array holds PXRB_NOALLOC_RHO_MAX doubles of rho (jobs of at most
+//    1,048,576 cells, e.g. 96^3 or 128x128x64) plus the partial sums; larger
+//    jobs are rejected with PXRB_ETOOLARGE before any GPU work;
+//  * every GPU that loads the library holds the array (~8.1 MiB) until exit;
+//  * every call shares the array and it keeps the last call's contents, so
+//    calls that overlap on the GPU (different streams, or a second call
+//    enqueued before the first finished, from any thread) race;
+//  * the first call on a device resolves the array's device address with
+//    cudaGetSymbolAddress (once per device); make that first call before any
+//    stream capture.
+// ---------------------------------------------------------------------------
+#define PXRB_NOALLOC_RHO_MAX (1 << 20)
+#define PXRB_NOALLOC_PART_MAX (8 * 1184)
+static __device__ __align__(256) double g_noalloc_scratch[PXRB_NOALLOC_RHO_MAX + PXRB_NOALLOC_PART_MAX];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_addr[256];   // per device; host-side copy of the device address
+
+extern "C" int pxrb_tiled_diagnostics_noalloc(const pxrb_tiled_job* job_host, int32_t gauss,
+                                              double* out, void* stream) {
+  if (!job_host || !out) return PXRB_EINVAL;
+  const Job& J = *job_host;
+  const i64 ncell = (i64)J.nx * J.ny * J.nz;
+  const int nb = diag_blocks(J);
+  if (ncell > PXRB_NOALLOC_RHO_MAX || 8 * nb > PXRB_NOALLOC_PART_MAX) return PXRB_ETOOLARGE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return PXRB_ELAUNCH;
+  double* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PXRB_ELAUNCH;
+      g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    base = g_noalloc_addr[dev];
+  }
+  double* rho = gauss ? base : nullptr;
+  double* part = base + PXRB_NOALLOC_RHO_MAX;
+  return pxrb_tiled_diagnostics(job_host, rho, part, PXRB_NOALLOC_PART_MAX, out, stream);
+}

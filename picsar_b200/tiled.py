@@ -58,6 +58,7 @@ _lib.register({
     "pxrb_tiled_smem_bytes": "=i I I I I I I I",
     "pxrb_tiled_job_size": "=i",
     "pxrb_tiled_diag_scratch": "=i p",
+    "pxrb_tiled_diagnostics_noalloc": "p I p s",
 })
 
 
@@ -320,6 +321,22 @@ class TiledSim:
         if not to_host:
             return self.diag_out
         o = self.diag_out.cpu().tolist()
+        return {"kinetic": o[0], "ex": o[1], "ey": o[2], "ez": o[3], "bx": o[4], "by": o[5],
+                "bz": o[6], "gauss_norm": o[7], "rho_norm": o[8], "field": sum(o[1:7]),
+                "total": o[0] + sum(o[1:7])}
+
+    def diagnostics_noalloc(self, gauss=True, out=None):
+        """Same values as diagnostics(), computed by the entry point that
+        allocates nothing (its scratch is a static device array of the
+        library; jobs up to 1,048,576 cells).  out: optional DEVICE float64[9]
+        tensor that receives the values."""
+        if out is None:
+            out = self.diag_out
+        if gauss:
+            self._pull_job()
+        _lib.call("pxrb_tiled_diagnostics_noalloc", self._jp(), int(bool(gauss)),
+                  out.data_ptr(), _stream())
+        o = out.cpu().tolist()
         return {"kinetic": o[0], "ex": o[1], "ey": o[2], "ez": o[3], "bx": o[4], "by": o[5],
                 "bz": o[6], "gauss_norm": o[7], "rho_norm": o[8], "field": sum(o[1:7]),
                 "total": o[0] + sum(o[1:7])}
