@@ -7,15 +7,15 @@
 // tests, the smoke check and the CPU-baseline leg of the benchmark load it;
 // no product code path links, imports or calls it.
 //
-// Parity status: the reference ships no golden vectors for this path and its
+// Parity status: PINNED.  The reference ships no golden vectors and its
 // Fortran cannot be compiled in this image (no Fortran compiler), so the
-// restatement is "parity unpinned" at the data level.  It is pinned instead by
-// (1) following the Fortran text line by line (loop order, parenthesisation,
-// intrinsic semantics: FLOOR -> floor, NINT -> round-half-away-from-zero),
-// and (2) reproducing the reference's own cross-variant checks and physics
-// invariants (specialised vs arbitrary-order Esirkepov, fused vs separate
-// gather, tiled vs untiled deposition, charge continuity, energy, plane
-// wave) in the test-suite.
+// reference's own routines are translated statement by statement to C
+// (oracle/ftrans.py: same types, loop bounds, operation order and intrinsic
+// semantics) and every kernel restated here is checked bit for bit against
+// them (tests/test_oracle_vs_reference.py): pushers, fused gather+push 1-3,
+// scalar gathers, Esirkepov 1-3 and _n, charge deposition, Yee.  The
+// reference's cross-variant checks and physics invariants are reproduced on
+// top (tests/test_oracle_cpu.py).
 //
 // Array convention: every grid is a Fortran column-major array with lower
 // bound -g and upper bound n+g per axis (x fastest), passed as a base pointer

@@ -145,3 +145,33 @@ def test_tiled_diagnostics_match_oracle(cuda):
     do, dt = o.diags(), t.diagnostics()
     for k in ("kinetic", "ex", "ey", "ez", "bx", "by", "bz", "gauss_norm"):
         assert abs(dt[k] - do[k]) <= 1e-10 * max(abs(do[k]), 1e-30), (k, dt[k], do[k])
+
+
+def test_golden_fixtures_fp64(cuda):
+    """FP64 tiled engine against the committed golden fixtures (made by the
+    oracle, tests/golden/make_golden.py), at 1e-12 relative L2."""
+    from tests.golden import make_golden as MG
+    fx = np.load(MG.PATH)
+    for case in MG.CASES:
+        tag = MG.tag(**case)
+        n, g = case["n"], MG.G
+        _, fields = MG.initial_state(case["n"], case["ppc"], case["sigma"], case["seed"])
+        t = TiledSim(n, order=case["order"], pusher=case["pusher"], precision="fp64",
+                     config=TiledConfig(tile=(8, 8, 8), sort_interval=1), track_ids=True)
+        for name, a in zip(FIELDS, fields):
+            t.import_field(name, P.to_fortran(a), g)
+        init = [fx[f"{tag}/init_{c}"] for c in ("x", "y", "z", "ux", "uy", "uz", "w")]
+        t.load_particles(*init)
+        t.step(case["steps"], keep_j=True)
+        torch.cuda.synchronize()
+        for name in MG.FIELDS:
+            err = rel_l2(t.export_field(name, g).cpu().numpy(), fx[f"{tag}/{name}"])
+            assert err <= 1e-12, (tag, name, err)
+        got = {k: v.cpu().numpy() for k, v in t.particles().items()}
+        for c in ("ux", "uy", "uz", "gaminv"):
+            err = rel_l2(got[c], fx[f"{tag}/{c}"])
+            assert err <= 1e-12, (tag, c, err)
+        for c, L in zip(("x", "y", "z"), n):
+            ref = fx[f"{tag}/{c}"]
+            dxp = (got[c] - ref + L / 2) % L - L / 2
+            assert np.linalg.norm(dxp) / np.linalg.norm(ref) <= 1e-12, (tag, c)
