@@ -193,6 +193,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload in ("ensemble", "serve"):
+        return run_reference_jobs(args)
     wl = WORKLOADS[args.workload]
     threads = os.cpu_count()
     rate, el, np_, nth = cpu_oracle_rate(wl, args.steps, args.warmup, threads)
@@ -210,6 +212,48 @@ def run_reference(args):
                 "d2h_bytes_per_step": 0},
         "note": "PICSAR's Fortran cannot be compiled in this image (no Fortran compiler); "
                 "the reference arm runs the line-by-line C++ restatement of its routines",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_jobs(args):
+    """Reference arm of the ensemble / served workloads: the oracle (OpenMP
+    over tiles, all host cores) on a bounded sample of jobs of the same
+    distribution, each job its own simulation as the reference runs them."""
+    from oracle import oracle as O
+    from picsar_b200.ensemble import ensemble_jobs
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    os.environ["OMP_NUM_THREADS"] = str(os.cpu_count())
+    specs = ensemble_jobs(count=args.jobs, seed=2024, steps=100)
+    sample = sorted(specs[:16], key=lambda sp: sp.particles)[:4]
+    steps = max(1, min(args.steps, 3))
+    ps, el_tot = 0, 0.0
+    for sp in sample:
+        st = sp.initial_state(device="cpu").numpy()
+        sim = O.OracleSim(sp.n, 3, order=sp.order, pusher=sp.pusher, tiles=(2, 2, 2),
+                          sorting_period=20)
+        sim.add_particles(st["x"], st["y"], st["z"], st["ux"], st["uy"], st["uz"], st["w"])
+        sim.step(1)
+        t0 = time.perf_counter()
+        sim.step(steps)
+        el_tot += time.perf_counter() - t0
+        ps += sp.particles * steps
+    rate = ps / el_tot
+    nth = O.num_threads()
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": rate,
+        "unit": "particle-steps/s", "n_gpus": ws, "steps": steps, "warmup": 1,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload,
+                   "sample": f"{len(sample)} smallest of the first 16 jobs, {steps} steps each"},
+        "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": nth, "kind": "port",
+                         "sample": f"{len(sample)} jobs x {steps} steps, OpenMP over tiles"},
+        "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -395,13 +439,198 @@ def run_plain_fp64(wl, args, ws, rank):
                     "particle, global FP64 atomics, separate bc kernels"}
 
 
+def _plain_fp64_jobs(specs, steps=2):
+    """Plain FP64 GPU path, one job at a time (PICSAR arrays, FP64 atomics):
+    per job 1 untimed step then `steps` timed steps (CUDA events).  Returns
+    (particle-steps/s over all jobs, {index: ms per step})."""
+    import torch
+    from picsar_b200.picsar import PicsarModule
+    per, tot_ps, tot_ms = {}, 0, 0.0
+    s = torch.cuda.current_stream()
+    for i, sp in enumerate(specs):
+        st = sp.initial_state(device="cuda")
+        m = PicsarModule(*sp.n, nguards=3, nox=sp.order, particle_pusher=sp.pusher)
+        m.add_species("electron", -1.0, 1.0, st.x, st.y, st.z, st.ux, st.uy, st.uz, st.w)
+        del st
+        m.step(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        m.step(steps)
+        b.record(s)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        per[i] = ms / steps
+        tot_ps += sp.particles * steps
+        tot_ms += ms
+        del m
+    torch.cuda.empty_cache()
+    return tot_ps / (tot_ms * 1e-3), per
+
+
+def _tuned_configs(specs, precision="fp32"):
+    from picsar_b200 import autotune
+    t0 = time.perf_counter()
+    tuned = autotune.tune_ensemble(specs, precision)
+    dt = time.perf_counter() - t0
+    info = {str(o): {"tile": r.config.tile[0], "drift": r.config.drift,
+                     "threads": r.config.threads, "sort_interval": r.config.sort_interval,
+                     "proxy_rate": r.rate, "ppc": r.ppc, "sigma": r.sigma, "cached": r.cached}
+            for o, r in tuned.items()}
+    return {o: r.config for o, r in tuned.items()}, info, dt
+
+
+def run_ensemble(args):
+    """Batched ensemble of uneven jobs (256 periodic thermal plasmas, cells
+    per axis U{16..96}, ppc in {1,2,4,8,16}, order in {1,2,3}, u_th
+    log-uniform 0.001-0.05, 100 steps each) in one persistent kernel set
+    replayed from CUDA graphs; autotuned per order; compared with the plain
+    FP64 path run job by job."""
+    import torch
+    from picsar_b200.ensemble import Ensemble, ensemble_jobs
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    total_steps = args.steps + args.warmup
+    specs = ensemble_jobs(count=args.jobs, seed=2024 + rank, steps=total_steps)
+    configs, tune_info, tune_s = _tuned_configs(specs)
+    ens = Ensemble(specs, "fp32", configs)
+    N = ens.particles_total
+    ens.step(args.warmup)
+    # kinetic energy is summed per tile by the particle kernel: read it after a step
+    d0 = ens.diagnostics()
+    pk_ms, yee_ms = ens.profile_steps(2)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    l0 = ens.launches
+    _barrier(ws)
+    clocks.start()
+    a.record(stream)
+    ens.step(args.steps)
+    b.record(stream)
+    _barrier(ws)
+    clk = clocks.stop()
+    ms = _max_over_ranks(a.elapsed_time(b), ws)
+    launches = ens.launches - l0
+    d1 = ens.diagnostics()
+    drift = [(y["total"] - x["total"]) / x["total"] for x, y in zip(d0, d1)]
+    value = N * ws * args.steps / (ms * 1e-3)
+    peak, peak_kind = _peaks()
+    alg = ens.algorithmic_bytes()
+    achieved = alg / (pk_ms * 1e-3) / 1e9
+    flags = ens.error_flags()
+    slow = ens.slow_path_count()
+    del ens
+    torch.cuda.empty_cache()
+    fp64 = None
+    if not args.skip_fp64:
+        sample = specs[::max(1, len(specs) // args.fp64_jobs)][:args.fp64_jobs]
+        rate64, _ = _plain_fp64_jobs(sample, steps=2)
+        fp64 = {"value": rate64 * ws, "unit": "particle-steps/s", "jobs_sampled": len(sample),
+                "what": "plain FP64 GPU path, jobs launched one at a time (sampled jobs, "
+                        "2 timed steps each after 1 untimed)"}
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"ensemble: {len(specs)} uneven periodic thermal-plasma jobs "
+                                   "(cells/axis U{16..96}, ppc {1,2,4,8,16}, order {1,2,3}, "
+                                   "u_th log-U[0.001,0.05]), one batched step per iteration "
+                                   "replayed from CUDA graphs",
+                       "particles_per_gpu": N, "jobs": len(specs),
+                       "precision": "FP32 mixed (FP64 J flush and energy sums)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": f"inputs larger than L2 (particle SoA {N * 32 / 1e9:.1f} GB), no flush",
+                       "autotuned": tune_info, "autotune_seconds": tune_s},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "k_tile_step (one launch per order group)",
+                         "kernel_ms": pk_ms, "yee_ms": yee_ms, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
+            "fp64_plain": fp64,
+            "speedup_vs_fp64_plain": value / fp64["value"] if fp64 else None,
+            "energy_drift": {"median_abs": float(statistics.median(abs(x) for x in drift)),
+                             "max_abs": float(max(abs(x) for x in drift))},
+            "error_flags": int(sum(flags)), "slow_path_particle_steps": slow,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def run_serve(args):
+    """Served stream: Poisson arrivals at each rate of --rates (jobs/s) of
+    jobs from the ensemble distribution with steps U{50..500}, admitted by
+    an HBM budget, continuously batched; p50/p99 latency and throughput,
+    against one-job-at-a-time plain FP64 execution (FIFO) of the same
+    stream, each job's service time measured on the plain FP64 path."""
+    import torch
+    from picsar_b200.ensemble import ensemble_jobs
+    from picsar_b200.serve import Server, fifo_latencies, percentile, poisson_requests
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    rates = [float(x) for x in args.rates.split(",")]
+    specs = ensemble_jobs(count=args.jobs, seed=77 + rank, steps_range=(50, 500))
+    configs, tune_info, tune_s = _tuned_configs(specs)
+    # warm-up: a few short jobs through the server (kernel attributes, pools)
+    warm = ensemble_jobs(count=6, seed=5, steps=3, cells=(16, 24))
+    Server("fp32", configs=configs).run(poisson_requests(warm, 1e6), clock="wall")
+    _, per_ms = _plain_fp64_jobs(specs, steps=2)
+    service = {i: per_ms[i] * specs[i].steps / 1e3 for i in range(len(specs))}
+    sweep = []
+    clocks = ClockSampler(local)
+    clocks.start()
+    for k, lam in enumerate(rates):
+        reqs = poisson_requests(specs, lam, seed=1000 + k)
+        rep = Server("fp32", hbm_budget=int(args.hbm_budget * 1e9), configs=configs).run(reqs)
+        s = rep.summary()
+        fifo = fifo_latencies(reqs, service)
+        fl = list(fifo.values())
+        fifo_span = max(r.arrival + fifo[r.rid] for r in reqs)
+        sweep.append({"rate_jobs_per_s": lam, **s,
+                      "fp64_fifo": {"p50_latency_s": percentile(fl, 50),
+                                    "p99_latency_s": percentile(fl, 99),
+                                    "particle_steps_per_s":
+                                        sum(sp.particles * sp.steps for sp in specs) / fifo_span}})
+    clk = clocks.stop()
+    if rank == 0:
+        top = max(sweep, key=lambda x: x["particle_steps_per_s"])
+        line = {
+            "metric": "particle-steps/s", "value": top["particle_steps_per_s"] * ws,
+            "unit": "particle-steps/s", "n_gpus": ws, "steps": None, "warmup": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"served stream: {len(specs)} jobs per rate from the ensemble "
+                                   "distribution, steps U{50..500}, Poisson arrivals, HBM budget "
+                                   f"{args.hbm_budget:g} GB, continuous batching",
+                       "rates_jobs_per_s": rates, "autotuned": tune_info,
+                       "autotune_seconds": tune_s},
+            "sweep": sweep, "clocks": clk,
+            "fp64_service_s_total": sum(service.values()),
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="large", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="large",
+                    choices=sorted(WORKLOADS) + ["ensemble", "serve"])
+    ap.add_argument("--jobs", type=int, default=None, help="ensemble / served jobs")
+    ap.add_argument("--fp64-jobs", type=int, default=24)
+    ap.add_argument("--rates", default="10,20,50,100,200")
+    ap.add_argument("--hbm-budget", type=float, default=150.0, help="GB")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--ctas-per-sm", type=int, default=2)
@@ -414,8 +643,16 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.steps is None:
+        args.steps = 95 if args.workload == "ensemble" else 200
+    if args.jobs is None:
+        args.jobs = 256 if args.workload == "ensemble" else 48
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ensemble":
+        return run_ensemble(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

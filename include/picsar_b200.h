@@ -286,6 +286,16 @@ int pxrb_tiled_push_e(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t pre
  * job_dev: the device copy the kernels read. */
 int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, void* stream);
 
+/* The same sort for a batch of jobs in five launches (an ensemble, the
+ * reference's per-species pxr_particle_sorting over many simulations).
+ * jobs_dev: DEVICE array of njobs descriptors, all of precision `prec`, each
+ * with cubic tiles of edge <= 8 and cell_cnt / rank_b set; max_tiles: at
+ * least the tile count of every job; max_np: the largest particle count
+ * (sizes the grid only).  The counters are cleared on the device, so the
+ * call needs no host copy of the descriptors. */
+int pxrb_tiled_sort_batch(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
+                          int32_t max_tiles, int64_t max_np, void* stream);
+
 /* Conversions between PICSAR's particle arrays (absolute FP64 positions,
  * u, weight; DEVICE) and the engine SoA of one job (unsorted after a load:
  * call pxrb_tiled_sort), and between PICSAR's guarded FP64 Fortran grids

@@ -1,0 +1,173 @@
+"""Autotuner of the tiled engine: cell-tile shape (edge and window margin),
+threads per tile CTA and sort interval, chosen by timing.
+
+For a (shape order, precision, particles per cell, thermal spread) class of
+jobs, a proxy simulation large enough to occupy every SM (at least two tiles
+per resident CTA) is stepped under each candidate and timed with CUDA events
+on the launching stream.  Stage 1 times every compiled (tile edge, margin)
+pair at both thread counts over 20 steps with a sort every 20 steps; stage 2
+times the winner at each sort interval over 40 steps (the slow path for
+particles that drifted out of their tile window, and the sort itself, both
+count).  Results are cached per GPU model in a JSON file
+(``$PICSAR_B200_CACHE`` or ``~/.cache/picsar_b200/autotune.json``).
+
+The reference has no autotuner: its tile counts, vector lengths and
+sorting period are deck parameters (src/parallelization/tiling/tiling.F90,
+src/housekeeping/sorting.F90).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+from dataclasses import asdict, dataclass, field
+
+import torch
+
+from .init import thermal_plasma
+from ._lib import PicsarB200Error
+from .tiled import SUPPORTED_SHAPES, TiledConfig, TiledSim
+
+THREADS = (128, 256)
+SORT_INTERVALS = (5, 10, 20, 40)
+
+
+@dataclass
+class TuneResult:
+    order: int
+    precision: str
+    ppc: int
+    sigma: float
+    config: TiledConfig
+    rate: float                     # particle-steps/s of the winner on the proxy
+    table: list = field(default_factory=list)   # (tile, drift, threads, sort, rate)
+    cached: bool = False
+
+
+def _cache_path():
+    p = os.environ.get("PICSAR_B200_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "picsar_b200", "autotune.json")
+
+
+def _key(order, precision, ppc, sigma, pusher):
+    name = torch.cuda.get_device_name()
+    sb = round(math.log10(max(sigma, 1e-6)) * 2) / 2
+    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}|p{pusher}"
+
+
+def proxy_grid(ppc, num_sms, tile=8, ctas_per_sm=2):
+    """Smallest grid of whole 8^3 tiles with at least two tiles per resident
+    CTA, x and y equal, at most ~12 M particles."""
+    need = 2 * num_sms * ctas_per_sm
+    nz_t = 8
+    nxy_t = max(4, math.ceil(math.sqrt(need / nz_t)))
+    n = (nxy_t * tile, nxy_t * tile, nz_t * tile)
+    while n[0] * n[1] * n[2] * ppc > 12_000_000 and n[2] > 16:
+        n = (n[0], n[1], n[2] // 2)
+    return n
+
+
+def _time(cfg, order, precision, st, n, steps, pusher):
+    sim = TiledSim(n, order=order, pusher=pusher, precision=precision, config=cfg)
+    sim.load_state(st)
+    sim.step(2)                                    # warm-up (kernel attributes)
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(s)
+    sim.step(steps)
+    b.record(s)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    rate = sim.np * steps / (ms * 1e-3)
+    del sim
+    return rate
+
+
+def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
+         shapes=None, threads=THREADS, sort_intervals=SORT_INTERVALS, seed=7):
+    """Best TiledConfig for jobs of this class, timed on a proxy simulation."""
+    path = _cache_path()
+    key = _key(order, precision, ppc, sigma, pusher)
+    if use_cache and os.path.exists(path):
+        try:
+            with open(path) as f:
+                c = json.load(f).get(key)
+            if c:
+                cfg = TiledConfig(**{**c["config"], "tile": tuple(c["config"]["tile"])})
+                return TuneResult(order, precision, ppc, sigma, cfg, c["rate"], c["table"],
+                                  cached=True)
+        except (OSError, ValueError, TypeError, KeyError):
+            pass
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    n = proxy_grid(ppc, props.multi_processor_count)
+    st = thermal_plasma(n, ppc, sigma, seed=seed, device="cuda")
+    if shapes is None:
+        shapes = sorted(SUPPORTED_SHAPES)
+    table = []
+    best = None
+    for edge, drift in shapes:
+        for th in threads:
+            cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, threads=th, sort_interval=20)
+            try:
+                r = _time(cfg, order, precision, st, n, 20, pusher)
+            except (ValueError, RuntimeError, PicsarB200Error) as e:   # not compiled here
+                table.append((edge, drift, th, 20, None, str(e)[:80]))
+                continue
+            table.append((edge, drift, th, 20, r))
+            if best is None or r > best[1]:
+                best = (cfg, r)
+    cfg0 = best[0]
+    best = None
+    for K in sort_intervals:
+        cfg = TiledConfig(tile=cfg0.tile, drift=cfg0.drift, threads=cfg0.threads, sort_interval=K)
+        r = _time(cfg, order, precision, st, n, 40, pusher)
+        table.append((cfg0.tile[0], cfg0.drift, cfg0.threads, K, r))
+        if best is None or r > best[1]:
+            best = (cfg, r)
+    res = TuneResult(order, precision, ppc, sigma, best[0], best[1], table)
+    if use_cache:
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            data = {}
+            if os.path.exists(path):
+                with open(path) as f:
+                    data = json.load(f)
+            data[key] = {"config": asdict(res.config), "rate": res.rate, "table": table}
+            with open(path, "w") as f:
+                json.dump(data, f, indent=1)
+        except (OSError, ValueError):
+            pass
+    return res
+
+
+def representative(specs):
+    """Per shape order: the particle-weighted median ppc and the 90th
+    percentile thermal spread of the jobs (the drift out of tile windows is
+    set by the fast tail)."""
+    out = {}
+    for o in (1, 2, 3):
+        js = [s for s in specs if s.order == o]
+        if not js:
+            continue
+        js_ppc = sorted(js, key=lambda s: s.ppc)
+        tot = sum(s.particles for s in js)
+        acc, ppc = 0, js_ppc[-1].ppc
+        for s in js_ppc:
+            acc += s.particles
+            if acc >= tot / 2:
+                ppc = s.ppc
+                break
+        sig = sorted(s.sigma for s in js)
+        out[o] = (ppc, sig[min(len(sig) - 1, int(0.9 * len(sig)))], js[0].pusher)
+    return out
+
+
+def tune_ensemble(specs, precision="fp32", use_cache=True):
+    """{order: TiledConfig} for an ensemble, one tuning per order present."""
+    res = {}
+    for o, (ppc, sig, pusher) in representative(specs).items():
+        res[o] = tune(o, precision, ppc=ppc, sigma=sig, pusher=pusher, use_cache=use_cache)
+    return res

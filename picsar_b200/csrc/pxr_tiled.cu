@@ -20,6 +20,7 @@
 
 #include <cub/block/block_scan.cuh>
 #include <mutex>
+#include <algorithm>
 
 namespace pxrt {
 int launch_order1(int, int, int, int, const pxrb_tiled_job*, const int2*, int, const int*, int*, int, int, size_t, cudaStream_t);
@@ -132,8 +133,21 @@ __device__ __forceinline__ int tile_of(const Job& J, uint32_t cell) {
   return i / J.tx + J.ntx * (j / J.ty + J.nty * (k / J.tz));
 }
 
+// Clears the tile counters and per-cell counters of every job of a batch
+// (job = blockIdx.y), in place of the single-job path's memsets.
+__global__ void k_sort_zero(const Job* __restrict__ jp) {
+  const Job& J = jp[blockIdx.y];
+  const i64 ntiles = (i64)J.ntx * J.nty * J.ntz;
+  const i64 ncell = ntiles * J.tx * J.ty * J.tz;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < ncell + ntiles + 1;
+       i += (i64)gridDim.x * blockDim.x) {
+    if (i <= ntiles) J.tile_cnt[i] = 0;
+    else J.cell_cnt[i - ntiles - 1] = 0;
+  }
+}
+
 __global__ void k_sort_count(const Job* __restrict__ jp) {
-  const Job& J = *jp;
+  const Job& J = jp[blockIdx.y];
   const int ntiles = J.ntx * J.nty * J.ntz;
   for (i64 p = blockIdx.x * (i64)blockDim.x + threadIdx.x; p < J.np;
        p += (i64)gridDim.x * blockDim.x) {
@@ -154,7 +168,7 @@ __global__ void __launch_bounds__(SCAN_TPB) k_sort_scan(const Job* __restrict__ 
   typedef cub::BlockScan<int, SCAN_TPB> Scan;
   __shared__ typename Scan::TempStorage tmp;
   __shared__ int carry;
-  const Job& J = *jp;
+  const Job& J = jp[blockIdx.y];
   const int ntiles = J.ntx * J.nty * J.ntz;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
@@ -174,7 +188,7 @@ __global__ void __launch_bounds__(SCAN_TPB) k_sort_scan(const Job* __restrict__ 
 
 template <typename R>
 __global__ void k_sort_scatter(const Job* __restrict__ jp) {
-  const Job& J = *jp;
+  const Job& J = jp[blockIdx.y];
   const R *ox = (const R*)J.ox, *oy = (const R*)J.oy, *oz = (const R*)J.oz;
   const R *ux = (const R*)J.ux, *uy = (const R*)J.uy, *uz = (const R*)J.uz, *w = (const R*)J.w;
   R *ox2 = (R*)J.ox_b, *oy2 = (R*)J.oy_b, *oz2 = (R*)J.oz_b;
@@ -223,9 +237,10 @@ constexpr int RR_MAXC = 512;     // cells per tile (tile edge <= 8)
 
 template <typename R>
 __global__ void __launch_bounds__(RR_TPB) k_sort_rr(const Job* __restrict__ jp) {
-  const Job& J = *jp;
+  const Job& J = jp[blockIdx.y];
   const int T = J.tx, T3 = T * T * T;
   const int t = blockIdx.x;
+  if (t >= J.ntx * J.nty * J.ntz) return;
   const int b0 = J.tile_off[t], b1 = J.tile_off[t + 1];
   if (b0 == b1) return;
   __shared__ int cnt[RR_MAXC], key[RR_MAXC], pos_of[RR_MAXC], cell_at[RR_MAXC];
@@ -614,6 +629,32 @@ int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, voi
       k_sort_scatter<double><<<nb, 256, 0, s>>>(job_dev);
       k_sort_rr<double><<<ntiles, RR_TPB, 0, s>>>(job_dev);
     }
+  }
+  PXRB_CHECK_LAUNCH();
+  return PXRB_OK;
+}
+
+int pxrb_tiled_sort_batch(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
+                          int32_t max_tiles, int64_t max_np, void* stream) {
+  if (!jobs_dev || njobs < 1 || njobs > 65535 || max_tiles < 1 || max_np < 0)
+    return PXRB_EINVAL;
+  if (prec < 0 || prec > 1) return PXRB_EUNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  // blocks per job: enough to cover the largest job, capped so that the whole
+  // batch stays a few thousand CTAs (each CTA strides through its job)
+  const int64_t want = (max_np + 255) / 256;
+  const int cap = njobs >= 4096 ? 1 : 4096 / njobs;
+  const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
+  const dim3 g_np(bx, njobs), g_one(1, njobs), g_tiles(max_tiles, njobs);
+  k_sort_zero<<<g_np, 256, 0, s>>>(jobs_dev);
+  k_sort_count<<<g_np, 256, 0, s>>>(jobs_dev);
+  k_sort_scan<<<g_one, SCAN_TPB, 0, s>>>(jobs_dev);
+  if (prec == 0) {
+    k_sort_scatter<float><<<g_np, 256, 0, s>>>(jobs_dev);
+    k_sort_rr<float><<<g_tiles, RR_TPB, 0, s>>>(jobs_dev);
+  } else {
+    k_sort_scatter<double><<<g_np, 256, 0, s>>>(jobs_dev);
+    k_sort_rr<double><<<g_tiles, RR_TPB, 0, s>>>(jobs_dev);
   }
   PXRB_CHECK_LAUNCH();
   return PXRB_OK;
