@@ -46,12 +46,30 @@ WORKLOADS = {
                    sigma=0.01, pusher=0,
                    desc="128x128x64 cells, 8 ppc (8,388,608 electrons), order 3, tiles 8^3, "
                         "re-sort every 20 steps, Boris, u_th 0.01, periodic (profiling size)"),
+    "uneven": dict(n=(512, 128, 128), ppc=16, order=2, tile=(8, 8, 8), sort_interval=20,
+                   sigma=0.005, u_drift=0.2, pusher=0, init="two_stream", autotune=True,
+                   tune_sigma=0.2,
+                   desc="512x128x128 cells, density ramp 0->1 over x in [0,256) then flat, "
+                        "16 ppc at n0 (~100.7 M electrons), two beams u_x=+-0.2 with u_th "
+                        "0.005, order 2, Boris, periodic, autotuned tiles and sort interval"),
     "plain-small": dict(n=(32, 32, 32), ppc=8, order=1, tile=(8, 8, 8), sort_interval=20,
                         sigma=0.01, pusher=0,
                         desc="32^3 cells, 8 ppc (262,144 electrons), order 1, Boris, u_th 0.01"),
 }
 BYTES_PER_PARTICLE = {0: (32 + 28), 1: (60 + 52)}        # particle kernel, per particle
 GRID_BYTES_PER_CELL = {0: (24 + 48), 1: (48 + 48)}        # E,B read + J FP64 read-modify-write
+
+
+def _initial_state(wl, seed, n=None, device="cuda"):
+    """Seeded synthetic initial plasma of a workload (optionally on a
+    smaller grid `n` with the same profile, for CPU samples)."""
+    from picsar_b200.init import thermal_plasma, two_stream_ramp
+    n = n or wl["n"]
+    if wl.get("init") == "two_stream":
+        ramp = max(1, round(256 * n[0] / wl["n"][0]))
+        return two_stream_ramp(n, wl["ppc"], wl["u_drift"], wl["sigma"], seed=seed,
+                               ramp_cells=ramp, device=device)
+    return thermal_plasma(n, wl["ppc"], wl["sigma"], seed=seed, device=device)
 
 
 def _peaks():
@@ -176,7 +194,9 @@ def cpu_oracle_rate(wl, steps, warmup, threads=None):
     n = (32, 32, 32)
     if threads:
         os.environ["OMP_NUM_THREADS"] = str(threads)
-    st = thermal_plasma(n, wl["ppc"], wl["sigma"], seed=11).numpy()
+    if wl.get("init") == "two_stream":
+        n = (64, 16, 16)
+    st = _initial_state(wl, 11, n=n, device="cpu").numpy()
     sim = O.OracleSim(n, 3, order=wl["order"], pusher=wl["pusher"], tiles=(4, 4, 4),
                       sorting_period=wl["sort_interval"])
     sim.add_particles(st["x"], st["y"], st["z"], st["ux"], st["uy"], st["uz"], st["w"])
@@ -271,11 +291,27 @@ def run_ours(args):
     prec = 0 if args.precision == "fp32" else 1
     cfg = TiledConfig(tile=wl["tile"], sort_interval=wl["sort_interval"], drift=1,
                       threads=args.threads, ctas_per_sm=args.ctas_per_sm, acc=args.acc)
-    st = thermal_plasma(wl["n"], wl["ppc"], wl["sigma"], seed=1234 + rank, device="cuda")
+    tuned = None
+    if wl.get("autotune"):
+        from picsar_b200 import autotune
+        r = autotune.tune(wl["order"], args.precision, ppc=wl["ppc"], sigma=wl["tune_sigma"],
+                          pusher=wl["pusher"])
+        cfg = TiledConfig(tile=r.config.tile, drift=r.config.drift, threads=r.config.threads,
+                          ctas_per_sm=args.ctas_per_sm, sort_interval=r.config.sort_interval,
+                          acc=args.acc)
+        tuned = {"proxy_rate": r.rate, "cached": r.cached}
+    st = _initial_state(wl, 1234 + rank)
     N = st.np
     sim = TiledSim(wl["n"], order=wl["order"], pusher=wl["pusher"], precision=args.precision,
                    config=cfg)
     sim.load_state(st)
+    cnt = (sim.tile_off[1:] - sim.tile_off[:-1]).double()
+    q = torch.quantile(cnt, torch.tensor([0.0, 0.1, 0.5, 0.9, 0.99, 1.0], dtype=torch.float64,
+                                         device=cnt.device)).tolist()
+    occupancy = {"particles_per_tile_p0_p10_p50_p90_p99_p100": q,
+                 "empty_tile_fraction": float((cnt == 0).double().mean()),
+                 "max_over_mean": float(cnt.max() / cnt.mean())}
+    del cnt
     for _ in range(args.warmup):
         sim.step(1)
     torch.cuda.synchronize()
@@ -322,12 +358,18 @@ def run_ours(args):
         e2e = run_e2e(sim, st, wl, args, ws)
     del st
 
+    del sim
+    torch.cuda.empty_cache()
     # plain FP64 GPU path on the same workload (the comparison baseline)
     fp64 = None
     if not args.skip_fp64:
-        del sim
-        torch.cuda.empty_cache()
         fp64 = run_plain_fp64(wl, args, ws, rank)
+
+    # FP32 mixed vs FP64 on the same state: one-step error, energy and
+    # Gauss-law drift over the run, for each pusher
+    accuracy = None
+    if not args.skip_accuracy and args.precision == "fp32":
+        accuracy = [run_accuracy(wl, args, p, cfg) for p in (0, 1)]
 
     cpu = None
     if rank == 0 and not args.skip_cpu:
@@ -349,7 +391,9 @@ def run_ours(args):
                              f"{N * 32 / 1e9:.1f} GB per GPU), no flush",
                        "tuning": {"tile": list(wl["tile"]), "drift": cfg.drift,
                                   "threads": cfg.threads, "ctas_per_sm": cfg.ctas_per_sm,
-                                  "sort_interval": cfg.sort_interval, "acc": cfg.acc}},
+                                  "sort_interval": cfg.sort_interval, "acc": cfg.acc,
+                                  "autotuned": tuned},
+                       "tile_occupancy": occupancy},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": f"k_tiled_step<{'float' if prec == 0 else 'double'},"
@@ -364,12 +408,68 @@ def run_ours(args):
             "energy": {"start": e0["total"], "end": e1["total"],
                        "rel_change": (e1["total"] - e0["total"]) / e0["total"]},
             "slow_path_particle_steps": slow,
+            "accuracy": accuracy,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def run_accuracy(wl, args, pusher, cfg):
+    """FP32 mixed against FP64 (the tiled FP64 engine, itself within 1e-12
+    of the oracle) from one identical state of the workload: relative L2
+    error of E, B and particle momenta after one step; total-energy drift
+    (from step 1, the first step with a kinetic energy sum) and Gauss-law
+    residual drift (from the loaded state) after `accuracy_steps` steps, in
+    both precisions."""
+    import torch
+    from picsar_b200.init import thermal_plasma
+    from picsar_b200.tiled import TiledConfig, TiledSim
+    cfg = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval, drift=cfg.drift,
+                      threads=cfg.threads)
+    st = _initial_state(wl, 4321)
+    steps = args.accuracy_steps
+    sims, one = {}, {}
+    t0 = time.perf_counter()
+    for prec in ("fp64", "fp32"):
+        t = TiledSim(wl["n"], order=wl["order"], pusher=pusher, precision=prec, config=cfg,
+                     track_ids=True)
+        t.load_state(st)
+        g0 = t.diagnostics(gauss=True)["gauss_norm"]
+        t.step(1)
+        d1 = t.diagnostics(gauss=False)
+        f = {n: t.export_field(n, 3) for n in ("ex", "ey", "ez", "bx", "by", "bz")}
+        pp = t.particles()
+        f.update({c: pp[c] for c in ("ux", "uy", "uz")})
+        del pp
+        one[prec] = f
+        sims[prec] = (t, g0, d1)
+    del st
+    err = {k: float(torch.linalg.norm(one["fp32"][k] - one["fp64"][k]) /
+                    torch.linalg.norm(one["fp64"][k])) for k in one["fp64"]}
+    del one
+    torch.cuda.empty_cache()
+    res = {"pusher": "Vay" if pusher else "Boris", "steps": steps,
+           "one_step_rel_l2_fp32_vs_fp64": err}
+    for prec, (t, g0, d1) in sims.items():
+        t.step(steps - 1)
+        d = t.diagnostics(gauss=True)
+        res[prec] = {"energy_drift": (d["total"] - d1["total"]) / d1["total"],
+                     "gauss_residual_start": g0, "gauss_residual_end": d["gauss_norm"],
+                     "gauss_residual_drift": abs(d["gauss_norm"] - g0) / g0,
+                     "error_flag": t.error_flag()}
+    e32, e64 = abs(res["fp32"]["energy_drift"]), abs(res["fp64"]["energy_drift"])
+    g32, g64 = res["fp32"]["gauss_residual_drift"], res["fp64"]["gauss_residual_drift"]
+    res["energy_drift_ratio_fp32_over_fp64"] = e32 / e64 if e64 else None
+    res["gauss_drift_fp32_minus_fp64"] = g32 - g64
+    res["gauss_residual_ratio_fp32_over_fp64"] = (res["fp32"]["gauss_residual_end"] /
+                                                  res["fp64"]["gauss_residual_end"])
+    res["seconds"] = time.perf_counter() - t0
+    del sims
+    torch.cuda.empty_cache()
+    return res
 
 
 def run_e2e(sim, st, wl, args, ws):
@@ -417,7 +517,7 @@ def run_plain_fp64(wl, args, ws, rank):
     import torch
     from picsar_b200.init import thermal_plasma
     from picsar_b200.picsar import PicsarModule
-    st = thermal_plasma(wl["n"], wl["ppc"], wl["sigma"], seed=1234 + rank, device="cuda")
+    st = _initial_state(wl, 1234 + rank)
     m = PicsarModule(*wl["n"], nguards=3, nox=wl["order"], particle_pusher=wl["pusher"])
     m.add_species("electron", -1.0, 1.0, st.x, st.y, st.z, st.ux, st.uy, st.uz, st.w)
     N = st.np
@@ -479,6 +579,39 @@ def _tuned_configs(specs, precision="fp32"):
     return {o: r.config for o, r in tuned.items()}, info, dt
 
 
+def _ensemble_accuracy(specs, configs, steps):
+    """The same jobs as an FP32 mixed and as an FP64 ensemble: per job the
+    total-energy drift from step 1 to the last step and the Gauss-law
+    residual at the end, FP32 against FP64."""
+    import torch
+    from picsar_b200.ensemble import Ensemble
+    out = {}
+    for prec, cfg in (("fp32", configs), ("fp64", None)):
+        ens = Ensemble(specs, prec, cfg)
+        g0 = [d["gauss_norm"] for d in ens.diagnostics(gauss=True)]
+        ens.step(1)
+        d1 = ens.diagnostics()
+        ens.step(steps - 1)
+        d2 = ens.diagnostics(gauss=True)
+        order = [id(sp) for sp, _ in ens.sims()]
+        out[prec] = {k: (abs((b["total"] - a["total"]) / a["total"]), b["gauss_norm"], g)
+                     for k, a, b, g in zip(order, d1, d2, g0)}
+        del ens
+        torch.cuda.empty_cache()
+    keys = list(out["fp64"])
+    er = [out["fp32"][k][0] / max(out["fp64"][k][0], 1e-300) for k in keys]
+    gr = [out["fp32"][k][1] / out["fp64"][k][1] for k in keys]
+    return {"jobs": len(keys), "steps": steps,
+            "energy_drift_fp32_median": float(statistics.median(out["fp32"][k][0] for k in keys)),
+            "energy_drift_fp64_median": float(statistics.median(out["fp64"][k][0] for k in keys)),
+            "energy_drift_ratio_median": float(statistics.median(er)),
+            "energy_drift_ratio_max": float(max(er)),
+            "jobs_within_2x_fp64_energy_drift": int(sum(
+                out["fp32"][k][0] <= 2 * out["fp64"][k][0] + 1e-7 for k in keys)),
+            "gauss_residual_ratio_max": float(max(gr)),
+            "gauss_residual_ratio_min": float(min(gr))}
+
+
 def run_ensemble(args):
     """Batched ensemble of uneven jobs (256 periodic thermal plasmas, cells
     per axis U{16..96}, ppc in {1,2,4,8,16}, order in {1,2,3}, u_th
@@ -521,6 +654,9 @@ def run_ensemble(args):
     slow = ens.slow_path_count()
     del ens
     torch.cuda.empty_cache()
+    accuracy = None
+    if not args.skip_accuracy:
+        accuracy = _ensemble_accuracy(specs[::8][:32], configs, total_steps)
     fp64 = None
     if not args.skip_fp64:
         sample = specs[::max(1, len(specs) // args.fp64_jobs)][:args.fp64_jobs]
@@ -554,6 +690,7 @@ def run_ensemble(args):
             "energy_drift": {"median_abs": float(statistics.median(abs(x) for x in drift)),
                              "max_abs": float(max(abs(x) for x in drift))},
             "error_flags": int(sum(flags)), "slow_path_particle_steps": slow,
+            "accuracy": accuracy,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -640,11 +777,13 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.steps is None:
-        args.steps = 95 if args.workload == "ensemble" else 200
+        args.steps = {"ensemble": 95, "uneven": 500}.get(args.workload, 200)
     if args.jobs is None:
         args.jobs = 256 if args.workload == "ensemble" else 48
     if args.impl == "reference":
