@@ -296,9 +296,7 @@ def run_ours(args):
         from picsar_b200 import autotune
         r = autotune.tune(wl["order"], args.precision, ppc=wl["ppc"], sigma=wl["tune_sigma"],
                           pusher=wl["pusher"])
-        cfg = TiledConfig(tile=r.config.tile, drift=r.config.drift, threads=r.config.threads,
-                          ctas_per_sm=args.ctas_per_sm, sort_interval=r.config.sort_interval,
-                          acc=args.acc)
+        cfg = _with_acc({0: r.config}, args.acc)[0]
         tuned = {"proxy_rate": r.rate, "cached": r.cached}
     st = _initial_state(wl, 1234 + rank)
     N = st.np
@@ -428,7 +426,7 @@ def run_accuracy(wl, args, pusher, cfg):
     from picsar_b200.init import thermal_plasma
     from picsar_b200.tiled import TiledConfig, TiledSim
     cfg = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval, drift=cfg.drift,
-                      threads=cfg.threads)
+                      threads=cfg.threads, acc=cfg.acc)
     st = _initial_state(wl, 4321)
     steps = args.accuracy_steps
     sims, one = {}, {}
@@ -579,6 +577,18 @@ def _tuned_configs(specs, precision="fp32"):
     return {o: r.config for o, r in tuned.items()}, info, dt
 
 
+def _with_acc(configs, acc):
+    """Tuned configs with the requested FP32 accumulator mode (the tuner
+    times mode 2; mode 1 is compiled for 8^3 tiles with margin 1 only)."""
+    from picsar_b200.tiled import SUPPORTED_ACC, TiledConfig
+    out = {}
+    for o, c in configs.items():
+        a = acc if acc in SUPPORTED_ACC.get((c.tile[0], c.drift), (2,)) else 2
+        out[o] = TiledConfig(tile=c.tile, drift=c.drift, threads=c.threads,
+                             ctas_per_sm=c.ctas_per_sm, sort_interval=c.sort_interval, acc=a)
+    return out
+
+
 def _ensemble_accuracy(specs, configs, steps):
     """The same jobs as an FP32 mixed and as an FP64 ensemble: per job the
     total-energy drift from step 1 to the last step and the Gauss-law
@@ -625,6 +635,9 @@ def run_ensemble(args):
     total_steps = args.steps + args.warmup
     specs = ensemble_jobs(count=args.jobs, seed=2024 + rank, steps=total_steps)
     configs, tune_info, tune_s = _tuned_configs(specs)
+    configs = _with_acc(configs, args.acc)
+    for o, c in configs.items():
+        tune_info[str(o)]["acc"] = c.acc
     ens = Ensemble(specs, "fp32", configs)
     N = ens.particles_total
     ens.step(args.warmup)
@@ -713,6 +726,9 @@ def run_serve(args):
     rates = [float(x) for x in args.rates.split(",")]
     specs = ensemble_jobs(count=args.jobs, seed=77 + rank, steps_range=(50, 500))
     configs, tune_info, tune_s = _tuned_configs(specs)
+    configs = _with_acc(configs, args.acc)
+    for o, c in configs.items():
+        tune_info[str(o)]["acc"] = c.acc
     # warm-up: a few short jobs through the server (kernel attributes, pools)
     warm = ensemble_jobs(count=6, seed=5, steps=3, cells=(16, 24))
     Server("fp32", configs=configs).run(poisson_requests(warm, 1e6), clock="wall")
@@ -771,7 +787,10 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--ctas-per-sm", type=int, default=2)
-    ap.add_argument("--acc", type=int, default=2, help="FP32 current accumulator mode")
+    ap.add_argument("--acc", type=int, default=1,
+                    help="FP32 current accumulator: 1 int32 fixed point (default: energy drift "
+                         "and Gauss residual within 1e-3 of FP64's, one-step field error "
+                         "~1e-4), 2 two-word 64-bit fixed point (~1e-5, slower), 0 FP32")
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--skip-e2e", action="store_true")

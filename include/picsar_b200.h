@@ -266,7 +266,9 @@ int64_t pxrb_tiled_smem_bytes(int32_t order, int32_t prec, int32_t acc, int32_t 
  * push_b: B -= frac*dt*curl E.  push_e: E += c^2 dt curl B - c^2 mu0 dt J,
  * then J = 0 when zero_j != 0.  cell_off_dev: DEVICE int64[njobs+1], start of
  * each job in a flat cell index whose job segments are padded to multiples of
- * 256; total_cells = cell_off[njobs] (host value). */
+ * 1024 (PXRB_YEE_CELLS_PER_BLOCK); total_cells = cell_off[njobs] (host value),
+ * a multiple of 1024. */
+#define PXRB_YEE_CELLS_PER_BLOCK 1024
 int pxrb_tiled_push_b(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
                       const int64_t* cell_off_dev, int64_t total_cells, double frac,
                       void* stream);

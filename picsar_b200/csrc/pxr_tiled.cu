@@ -63,32 +63,70 @@ __device__ __forceinline__ void store_images(R* base, int i, int j, int k, int n
         base[(ii[a] + G) + (i64)pitch * ((jj[b] + G) + (i64)NYg * (kk[c] + G))] = v;
 }
 
+// Cell (i, j, k) of a job's flat cell index (x fastest).  The flat index of
+// one job is below 2^32 (2^32 cells of the engine's layout exceed any one
+// GPU's memory), so 32-bit divisions suffice.
+__device__ __forceinline__ void yee_ijk(int64_t lid, int nx, int ny, int& i, int& j, int& k) {
+  const uint32_t l = (uint32_t)lid, ux = (uint32_t)nx, uy = (uint32_t)ny;
+  const uint32_t t = l / ux;
+  i = (int)(l - t * ux);
+  const uint32_t kk = t / uy;
+  j = (int)(t - kk * uy);
+  k = (int)kk;
+}
+
+// Each thread updates YEE_CPT cells spaced by the block size, loading all of
+// them before computing (memory-level parallelism); a block covers YEE_CPB
+// consecutive cells of one job.
+constexpr int YEE_CPT = 4;
+constexpr int YEE_CPB = YEE_TPB * YEE_CPT;
+
 template <typename R>
 __global__ void __launch_bounds__(YEE_TPB)
     k_yee_b_t(const Job* __restrict__ jobs, int njobs, const int64_t* __restrict__ off, R frac) {
   __shared__ int s_job;
-  const int64_t gid0 = (int64_t)blockIdx.x * YEE_TPB;
-  if (threadIdx.x == 0) s_job = find_job(off, njobs, gid0);
+  __shared__ R s_c[3];
+  const int64_t gid0 = (int64_t)blockIdx.x * YEE_CPB;
+  if (threadIdx.x == 0) {
+    const int jb = find_job(off, njobs, gid0);
+    const Job& J0 = jobs[jb];
+    s_job = jb;
+    s_c[0] = (R)(frac * J0.dt / J0.dx);
+    s_c[1] = (R)(frac * J0.dt / J0.dy);
+    s_c[2] = (R)(frac * J0.dt / J0.dz);
+  }
   __syncthreads();
   const Job& J = jobs[s_job];
-  const int64_t lid = gid0 - off[s_job] + threadIdx.x;
+  const int64_t l0 = gid0 - off[s_job] + threadIdx.x;
   const int nx = J.nx, ny = J.ny, nz = J.nz;
-  if (lid >= (int64_t)nx * ny * nz) return;
-  const int i = (int)(lid % nx), j = (int)((lid / nx) % ny), k = (int)(lid / ((int64_t)nx * ny));
+  const int64_t ncell = (int64_t)nx * ny * nz;
   const int G = J.g, pitch = J.pitch_x, NYg = J.pitch_y;
   const i64 sy = pitch, sz = (i64)pitch * NYg;
-  const i64 c = (i + G) + sy * (j + G) + sz * (k + G);
   const R* ex = (const R*)J.ex; const R* ey = (const R*)J.ey; const R* ez = (const R*)J.ez;
   R* bx = (R*)J.bx; R* by = (R*)J.by; R* bz = (R*)J.bz;
-  const R dtsdx = (R)(frac * J.dt / J.dx), dtsdy = (R)(frac * J.dt / J.dy),
-          dtsdz = (R)(frac * J.dt / J.dz);
-  const R ezc = ez[c], eyc = ey[c], exc = ex[c];
-  R vbx = bx[c] - dtsdy * (ez[c + sy] - ezc) + dtsdz * (ey[c + sz] - eyc);
-  R vby = by[c] + dtsdx * (ez[c + 1] - ezc) - dtsdz * (ex[c + sz] - exc);
-  R vbz = bz[c] - dtsdx * (ey[c + 1] - eyc) + dtsdy * (ex[c + sy] - exc);
-  store_images(bx, i, j, k, nx, ny, nz, G, pitch, NYg, vbx);
-  store_images(by, i, j, k, nx, ny, nz, G, pitch, NYg, vby);
-  store_images(bz, i, j, k, nx, ny, nz, G, pitch, NYg, vbz);
+  const R dtsdx = s_c[0], dtsdy = s_c[1], dtsdz = s_c[2];
+  int ci[YEE_CPT], cj[YEE_CPT], ck[YEE_CPT];
+  R vbx[YEE_CPT], vby[YEE_CPT], vbz[YEE_CPT];
+#pragma unroll
+  for (int u = 0; u < YEE_CPT; ++u) {
+    const int64_t lid = l0 + u * YEE_TPB;
+    if (lid < ncell) {
+      yee_ijk(lid, nx, ny, ci[u], cj[u], ck[u]);
+      const i64 c = (ci[u] + G) + sy * (cj[u] + G) + sz * (ck[u] + G);
+      const R ezc = ez[c], eyc = ey[c], exc = ex[c];
+      vbx[u] = bx[c] - dtsdy * (ez[c + sy] - ezc) + dtsdz * (ey[c + sz] - eyc);
+      vby[u] = by[c] + dtsdx * (ez[c + 1] - ezc) - dtsdz * (ex[c + sz] - exc);
+      vbz[u] = bz[c] - dtsdx * (ey[c + 1] - eyc) + dtsdy * (ex[c + sy] - exc);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < YEE_CPT; ++u) {
+    if (l0 + u * YEE_TPB < ncell) {
+      store_images(bx, ci[u], cj[u], ck[u], nx, ny, nz, G, pitch, NYg, vbx[u]);
+      store_images(by, ci[u], cj[u], ck[u], nx, ny, nz, G, pitch, NYg, vby[u]);
+      store_images(bz, ci[u], cj[u], ck[u], nx, ny, nz, G, pitch, NYg, vbz[u]);
+    }
+  }
 }
 
 template <typename R>
@@ -96,32 +134,54 @@ __global__ void __launch_bounds__(YEE_TPB)
     k_yee_e_t(const Job* __restrict__ jobs, int njobs, const int64_t* __restrict__ off,
               int zero_j) {
   __shared__ int s_job;
-  const int64_t gid0 = (int64_t)blockIdx.x * YEE_TPB;
-  if (threadIdx.x == 0) s_job = find_job(off, njobs, gid0);
+  __shared__ R s_c[4];
+  const int64_t gid0 = (int64_t)blockIdx.x * YEE_CPB;
+  if (threadIdx.x == 0) {
+    const int jb = find_job(off, njobs, gid0);
+    const Job& J0 = jobs[jb];
+    s_job = jb;
+    const double c2 = J0.clight * J0.clight;
+    s_c[0] = (R)(c2 * J0.mu0 * J0.dt);
+    s_c[1] = (R)(c2 * J0.dt / J0.dx);
+    s_c[2] = (R)(c2 * J0.dt / J0.dy);
+    s_c[3] = (R)(c2 * J0.dt / J0.dz);
+  }
   __syncthreads();
   const Job& J = jobs[s_job];
-  const int64_t lid = gid0 - off[s_job] + threadIdx.x;
+  const int64_t l0 = gid0 - off[s_job] + threadIdx.x;
   const int nx = J.nx, ny = J.ny, nz = J.nz;
-  if (lid >= (int64_t)nx * ny * nz) return;
-  const int i = (int)(lid % nx), j = (int)((lid / nx) % ny), k = (int)(lid / ((int64_t)nx * ny));
+  const int64_t ncell = (int64_t)nx * ny * nz;
   const int G = J.g, pitch = J.pitch_x, NYg = J.pitch_y;
   const i64 sy = pitch, sz = (i64)pitch * NYg;
-  const i64 c = (i + G) + sy * (j + G) + sz * (k + G);
   R* ex = (R*)J.ex; R* ey = (R*)J.ey; R* ez = (R*)J.ez;
   const R* bx = (const R*)J.bx; const R* by = (const R*)J.by; const R* bz = (const R*)J.bz;
-  const double c2 = J.clight * J.clight;
-  const R mudt = (R)(c2 * J.mu0 * J.dt), dtsdx = (R)(c2 * J.dt / J.dx),
-          dtsdy = (R)(c2 * J.dt / J.dy), dtsdz = (R)(c2 * J.dt / J.dz);
-  const i64 jc = lid;
-  const R jxv = (R)J.jx[jc], jyv = (R)J.jy[jc], jzv = (R)J.jz[jc];
-  if (zero_j) { J.jx[jc] = 0.0; J.jy[jc] = 0.0; J.jz[jc] = 0.0; }
-  const R bzc = bz[c], byc = by[c], bxc = bx[c];
-  R vex = ex[c] + dtsdy * (bzc - bz[c - sy]) - dtsdz * (byc - by[c - sz]) - mudt * jxv;
-  R vey = ey[c] - dtsdx * (bzc - bz[c - 1]) + dtsdz * (bxc - bx[c - sz]) - mudt * jyv;
-  R vez = ez[c] + dtsdx * (byc - by[c - 1]) - dtsdy * (bxc - bx[c - sy]) - mudt * jzv;
-  store_images(ex, i, j, k, nx, ny, nz, G, pitch, NYg, vex);
-  store_images(ey, i, j, k, nx, ny, nz, G, pitch, NYg, vey);
-  store_images(ez, i, j, k, nx, ny, nz, G, pitch, NYg, vez);
+  double* jxp = J.jx; double* jyp = J.jy; double* jzp = J.jz;
+  const R mudt = s_c[0], dtsdx = s_c[1], dtsdy = s_c[2], dtsdz = s_c[3];
+  int ci[YEE_CPT], cj[YEE_CPT], ck[YEE_CPT];
+  R vex[YEE_CPT], vey[YEE_CPT], vez[YEE_CPT];
+#pragma unroll
+  for (int u = 0; u < YEE_CPT; ++u) {
+    const int64_t lid = l0 + u * YEE_TPB;
+    if (lid < ncell) {
+      yee_ijk(lid, nx, ny, ci[u], cj[u], ck[u]);
+      const i64 c = (ci[u] + G) + sy * (cj[u] + G) + sz * (ck[u] + G);
+      const R jxv = (R)jxp[lid], jyv = (R)jyp[lid], jzv = (R)jzp[lid];
+      const R bzc = bz[c], byc = by[c], bxc = bx[c];
+      vex[u] = ex[c] + dtsdy * (bzc - bz[c - sy]) - dtsdz * (byc - by[c - sz]) - mudt * jxv;
+      vey[u] = ey[c] - dtsdx * (bzc - bz[c - 1]) + dtsdz * (bxc - bx[c - sz]) - mudt * jyv;
+      vez[u] = ez[c] + dtsdx * (byc - by[c - 1]) - dtsdy * (bxc - bx[c - sy]) - mudt * jzv;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < YEE_CPT; ++u) {
+    const int64_t lid = l0 + u * YEE_TPB;
+    if (lid < ncell) {
+      if (zero_j) { jxp[lid] = 0.0; jyp[lid] = 0.0; jzp[lid] = 0.0; }
+      store_images(ex, ci[u], cj[u], ck[u], nx, ny, nz, G, pitch, NYg, vex[u]);
+      store_images(ey, ci[u], cj[u], ck[u], nx, ny, nz, G, pitch, NYg, vey[u]);
+      store_images(ez, ci[u], cj[u], ck[u], nx, ny, nz, G, pitch, NYg, vez[u]);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -582,9 +642,10 @@ int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int3
 int pxrb_tiled_push_b(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
                       const int64_t* cell_off_dev, int64_t total_cells, double frac,
                       void* stream) {
-  if (!jobs_dev || !cell_off_dev || njobs < 1 || total_cells < 0) return PXRB_EINVAL;
+  if (!jobs_dev || !cell_off_dev || njobs < 1 || total_cells < 0 || total_cells % YEE_CPB)
+    return PXRB_EINVAL;
   if (total_cells == 0) return PXRB_OK;
-  int nb = (int)((total_cells + YEE_TPB - 1) / YEE_TPB);
+  int nb = (int)(total_cells / YEE_CPB);
   cudaStream_t s = (cudaStream_t)stream;
   if (prec == 0) k_yee_b_t<float><<<nb, YEE_TPB, 0, s>>>(jobs_dev, njobs, cell_off_dev, (float)frac);
   else k_yee_b_t<double><<<nb, YEE_TPB, 0, s>>>(jobs_dev, njobs, cell_off_dev, frac);
@@ -595,9 +656,10 @@ int pxrb_tiled_push_b(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t pre
 int pxrb_tiled_push_e(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
                       const int64_t* cell_off_dev, int64_t total_cells, int32_t zero_j,
                       void* stream) {
-  if (!jobs_dev || !cell_off_dev || njobs < 1 || total_cells < 0) return PXRB_EINVAL;
+  if (!jobs_dev || !cell_off_dev || njobs < 1 || total_cells < 0 || total_cells % YEE_CPB)
+    return PXRB_EINVAL;
   if (total_cells == 0) return PXRB_OK;
-  int nb = (int)((total_cells + YEE_TPB - 1) / YEE_TPB);
+  int nb = (int)(total_cells / YEE_CPB);
   cudaStream_t s = (cudaStream_t)stream;
   if (prec == 0) k_yee_e_t<float><<<nb, YEE_TPB, 0, s>>>(jobs_dev, njobs, cell_off_dev, zero_j);
   else k_yee_e_t<double><<<nb, YEE_TPB, 0, s>>>(jobs_dev, njobs, cell_off_dev, zero_j);

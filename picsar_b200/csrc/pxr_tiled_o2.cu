@@ -34,7 +34,9 @@ int launch_shape(int tile, int drift, int mode, const Job* jobs, const int2* wor
     PXRB_TD(8, 1, 0)
     PXRB_TD(8, 0, 2)
     PXRB_TD(8, 2, 2)
+    PXRB_TD(8, 2, 1)
     PXRB_TD(4, 1, 2)
+    PXRB_TD(4, 1, 1)
     PXRB_TD(4, 0, 2)
   }
 #undef PXRB_TD

@@ -210,7 +210,7 @@ class Ensemble:
             k = e
         offs = [0]
         for sp, sim in self.members:
-            offs.append(offs[-1] + -(-sp.cells // 256) * 256)
+            offs.append(offs[-1] + -(-sp.cells // 1024) * 1024)
         self.total_cells = offs[-1]
         self.cell_off = torch.tensor(offs, dtype=torch.int64, device=self.device)
         self.particles_total = sum(sim.np for _, sim in self.members)

@@ -77,7 +77,7 @@ _I32MAX = 2 ** 31 - 1
 # (tile edge, window margin) pairs the particle kernel is compiled for
 SUPPORTED_SHAPES = {(8, 1), (8, 0), (8, 2), (4, 1), (4, 0)}
 # accumulator modes compiled for the FP32 engine per shape (FP64 engine: mode 3)
-SUPPORTED_ACC = {(8, 1): (0, 1, 2)}
+SUPPORTED_ACC = {(8, 1): (0, 1, 2), (8, 2): (1, 2), (4, 1): (1, 2)}
 
 
 @dataclass
@@ -149,7 +149,7 @@ class TiledSim:
                                  torch.arange(self.ntiles, dtype=torch.int32)], 1).contiguous().to(dev)
         self.ctr = torch.zeros(1, dtype=torch.int32, device=dev)
         ncell = nx * ny * nz
-        self.total_cells = -(-ncell // 256) * 256
+        self.total_cells = -(-ncell // 1024) * 1024
         self.cell_off = torch.tensor([0, self.total_cells], dtype=torch.int64, device=dev)
         self.diag_out = torch.zeros(9, dtype=torch.float64, device=dev)
         self.track_ids = track_ids
