@@ -57,6 +57,24 @@ WORKLOADS = {
                         desc="32^3 cells, 8 ppc (262,144 electrons), order 1, Boris, u_th 0.01"),
 }
 BYTES_PER_PARTICLE = {0: (32 + 28), 1: (60 + 52)}        # particle kernel, per particle
+# Shared-memory work of the fused particle kernel per particle (FP32 engine):
+# energy-conserving gather points (E: 3*S*N*N, B: 3*N*S*S; N = order+1,
+# S = order) and fast-path Esirkepov accumulator updates (3*(N-1)*N*N, per
+# fixed-point word).  Conflict-free shared-memory rates of this pool's B200,
+# warp-instructions per clock per SM, measured with a 32-bit load / 32-bit
+# atomic-add probe at 8-64 resident warps: LDS.32 0.88, ATOMS.32 0.61.
+GATHER_POINTS = {1: 18, 2: 90, 3: 252}
+DEPOSIT_UPDATES = {1: 12, 2: 54, 3: 144}
+SMEM_RATE = {"lds": 0.88, "atoms": 0.61}
+
+
+def smem_floor_ms(order, acc, particles, sms, clock_mhz):
+    """Lower bound of the fused particle kernel's time set by shared-memory
+    instruction throughput (loads and accumulator atomics, conflict-free)."""
+    words = 2 if acc == 2 else 1
+    clk_per_warp = (GATHER_POINTS[order] / SMEM_RATE["lds"] +
+                    DEPOSIT_UPDATES[order] * words / SMEM_RATE["atoms"])
+    return particles / 32.0 * clk_per_warp / sms / (clock_mhz * 1e6) * 1e3
 GRID_BYTES_PER_CELL = {0: (24 + 48), 1: (48 + 48)}        # E,B read + J FP64 read-modify-write
 
 
@@ -398,6 +416,7 @@ def run_ours(args):
                                    f"{wl['order']}>",
                          "kernel_ms": kern_ms, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},
+            "smem_roofline": _smem_roofline(wl, prec, cfg, N, kern_ms, clk),
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
@@ -413,6 +432,19 @@ def run_ours(args):
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def _smem_roofline(wl, prec, cfg, N, kern_ms, clk):
+    if prec != 0:
+        return None
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    floor = smem_floor_ms(wl["order"], cfg.acc, N, sms, mhz)
+    return {"bound": "shared-memory instructions", "floor_ms": floor, "kernel_ms": kern_ms,
+            "frac": floor / kern_ms, "gather_points": GATHER_POINTS[wl["order"]],
+            "accumulator_updates": DEPOSIT_UPDATES[wl["order"]] * (2 if cfg.acc == 2 else 1),
+            "rates_warp_inst_per_clk_sm": SMEM_RATE, "sm_mhz": mhz}
 
 
 def run_accuracy(wl, args, pusher, cfg):
