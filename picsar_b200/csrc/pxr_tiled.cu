@@ -597,8 +597,7 @@ int64_t smem_bytes(int order, int prec, int acc, int tx, int ty, int tz, int dri
   i64 V = (i64)(tx + 2 * drift + lh) * (ty + 2 * drift + lh) * (tz + 2 * drift + lh);
   i64 r = prec ? 8 : 4;
   i64 a = acc == 3 ? 8 : 4, nw = acc == 2 ? 2 : 1;
-  const i64 qcap = (prec == 0 && acc != 2) ? 512 : 256;   // pxrt::QCap
-  return V * (6 * r + 3 * a * nw) + qcap * (3 * r + 8);
+  return V * (6 * r + 3 * a * nw);
 }
 
 inline int gs_blocks(i64 n, int tpb) {

@@ -411,15 +411,6 @@ __device__ __forceinline__ void dep_window_same(typename Acc<MODE>::T* base, con
   }
 }
 
-// General window deposit (a node changes along some axis), kept out of line.
-template <int ORDER, typename R, int MODE, int SY, int SZ, int V>
-__device__ __noinline__ void dep_window_general(typename Acc<MODE>::T* Js,
-                                                const EsirAxis<ORDER, R>& X,
-                                                const EsirAxis<ORDER, R>& Y,
-                                                const EsirAxis<ORDER, R>& Z, R cx, R cy, R cz) {
-  dep_window<ORDER, R, MODE, SY, SZ, V>(Js, X, Y, Z, cx, cy, cz);
-}
-
 // Global variant (particles outside their tile window): FP64 atomics on the
 // periodic J grid, in the reference's W-prefix form (unscaled coefficients).
 template <int ORDER, typename R>
@@ -466,15 +457,13 @@ __device__ __forceinline__ R gwin(const R* base, const R* sa, const R* sb, const
 }
 
 constexpr int MAX_THREADS = 256;
-// Per-tile queue of window particles whose node changes along some axis: they
-// are deposited after the tile's main loop by full warps, so the common
-// same-node path never diverges into the general one.
-constexpr int QCAP = 256;
-// Queue capacity of an instantiation: 512 entries where shared memory still
-// allows two CTAs per SM (FP32 engine, one-word accumulators), else 256.
-template <typename R, int MODE> struct QCap {
-  static constexpr int value = (sizeof(R) == 4 && MODE != 2) ? 512 : 256;
-};
+// Window particles whose Esirkepov node changes along some axis are queued
+// and deposited after the tile's main loop by full warps, so the common
+// same-node path never diverges into the general one.  The queue lives in
+// the sort's scratch buffers, free between sorts: the tile's own range of
+// rank_b lists the queued particles, and each queued particle's slot of
+// ox_b/oy_b/oz_b and cell_b holds its old offsets and packed box - so the
+// queue holds every particle of the tile and cannot overflow.
 
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
@@ -499,15 +488,10 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* Fs = reinterpret_cast<R*>(smem_raw);
   A* Js = reinterpret_cast<A*>(smem_raw + (size_t)6 * V * sizeof(R));
-  unsigned char* qbase = smem_raw + (size_t)6 * V * sizeof(R) + (size_t)3 * V * Acc<MODE>::NW * sizeof(A);
-  constexpr int QC = QCap<R, MODE>::value;
-  R* q_o = reinterpret_cast<R*>(qbase);                                 // [3][QC]
-  int* q_ip = reinterpret_cast<int*>(qbase + 3 * QC * sizeof(R));        // [QC]
-  unsigned* q_pk = reinterpret_cast<unsigned*>(q_ip + QC);               // [QC]
   __shared__ Job sj;
   __shared__ int s_item;
   __shared__ int s_qn;
-  __shared__ float s_max[6][MAX_THREADS / 32];
+  __shared__ float s_max[5][MAX_THREADS / 32];
   __shared__ double s_red[MAX_THREADS / 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 
@@ -564,7 +548,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     // A node of the window receives deposits only from particles whose old
     // cell lies within L+H+3 cells of it along every axis, so the node sum
     // is bounded by (max particles per window cell) * (L+H+3)^3 contributions.
-    float umax2 = 0.f, wmax = 0.f, cmax = 0.f, usum = 0.f;
+    float umax2 = 0.f, wmax = 0.f, cmax = 0.f;
     constexpr bool FIXED = MODE == 1 || MODE == 2;
     if (FIXED) {
       int* hist = reinterpret_cast<int*>(Js) + 2 * V;   // zero; re-zeroed below
@@ -574,7 +558,6 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
         float a = (float)uxp[ip], b = (float)uyp[ip], c = (float)uzp[ip];
         umax2 = fmaxf(umax2, a * a + b * b + c * c);
-        usum += fabsf(a) + fabsf(b) + fabsf(c);
         wmax = fmaxf(wmax, fabsf((float)wp[ip]));
         int ci, cj, ck;
         unpack_cell(sj.cell[ip], ci, cj, ck);
@@ -594,25 +577,18 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     }
     emax = warp_max(emax); bmax = warp_max(bmax); umax2 = warp_max(umax2); wmax = warp_max(wmax);
     cmax = warp_max(cmax);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) usum += __shfl_xor_sync(0xffffffffu, usum, off);
     if (lane == 0) {
       s_max[0][wid] = emax; s_max[1][wid] = bmax; s_max[2][wid] = umax2; s_max[3][wid] = wmax;
-      s_max[4][wid] = cmax; s_max[5][wid] = usum;
+      s_max[4][wid] = cmax;
     }
     __syncthreads();
     double scale[3];
     scale[0] = scale[1] = scale[2] = 1.0;
-    // A tile is "hot" when its expected number of node-changing particles
-    // (particles x 3 x largest per-step displacement in cells) could fill
-    // the queue: its particle loop then drains the queue between rounds.
-    bool hot = false;
     if (FIXED) {
-      float E = 0.f, B = 0.f, U2 = 0.f, Wm = 0.f, Cm = 0.f, Us = 0.f;
+      float E = 0.f, B = 0.f, U2 = 0.f, Wm = 0.f, Cm = 0.f;
       for (int w = 0; w < nwarps; ++w) {
         E = fmaxf(E, s_max[0][w]); B = fmaxf(B, s_max[1][w]);
         U2 = fmaxf(U2, s_max[2][w]); Wm = fmaxf(Wm, s_max[3][w]); Cm = fmaxf(Cm, s_max[4][w]);
-        Us += s_max[5][w];
       }
       const double c = sj.clight;
       const double ub = sqrt((double)U2) +
@@ -621,14 +597,6 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       const double dV = sj.dx * sj.dy * sj.dz;
       constexpr int reach = L + H + 3;
       const double np_ = fmax((double)Cm * (reach * reach * reach), 1.0);
-      {
-        // expected node changes ~ sum over particles and axes of |v| dt / d
-        // (|v| <= |u|), plus the push's change of u over the step
-        const double dmin = fmin(sj.dx, fmin(sj.dy, sj.dz));
-        const double du = fabs(sj.q) / sj.m * sj.dt * ((double)E + c * B);
-        const double expect = ((double)Us + 3.0 * du * (pend - pbeg)) * sj.dt / dmin;
-        hot = expect > 0.5 * QC;
-      }
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const double dq = q == 0 ? sj.dx : (q == 1 ? sj.dy : sj.dz);
@@ -652,42 +620,14 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     R *oxp = (R*)sj.ox, *oyp = (R*)sj.oy, *ozp = (R*)sj.oz;
     R *uxp = (R*)sj.ux, *uyp = (R*)sj.uy, *uzp = (R*)sj.uz;
     const R* wp = (const R*)sj.w;
+    int* q_list = sj.rank_b;
+    uint32_t* q_pk = sj.cell_b;
+    R *q_ox = (R*)sj.ox_b, *q_oy = (R*)sj.oy_b, *q_oz = (R*)sj.oz_b;
     double ke = 0.0;
     int nslow = 0, bad = 0;
     __syncthreads();
 
-    // deposit of queued window particles that changed node (full warps)
-    auto flush_queue = [&]() {
-      const int nq = min(s_qn, QC);
-      for (int q = threadIdx.x; q < nq; q += blockDim.x) {
-        const int ip = q_ip[q];
-        const unsigned pk = q_pk[q];
-        const int bx = pk & 255u, by = (pk >> 8) & 255u, bz = (pk >> 16) & 255u;
-        const int sx = (int)((pk >> 24) & 3u) - 1, sy = (int)((pk >> 26) & 3u) - 1,
-                  sz = (int)((pk >> 28) & 3u) - 1;
-        const R ox = q_o[q], oy = q_o[QC + q], oz = q_o[2 * QC + q];
-        const R nox = oxp[ip], noy = oyp[ip], noz = ozp[ip], wq = wp[ip];
-        int r0, r1;
-        R a0, a1;
-        EsirAxis<ORDER, R> EX, EY, EZ;
-        esir_node<ORDER, R>(nox, r0, a0); esir_node<ORDER, R>(ox, r1, a1);
-        bool ok = EX.set(bx + sx + r0, a0, bx + r1, a1);
-        esir_node<ORDER, R>(noy, r0, a0); esir_node<ORDER, R>(oy, r1, a1);
-        ok = EY.set(by + sy + r0, a0, by + r1, a1) && ok;
-        esir_node<ORDER, R>(noz, r0, a0); esir_node<ORDER, R>(oz, r1, a1);
-        ok = EZ.set(bz + sz + r0, a0, bz + r1, a1) && ok;
-        if (!ok) bad = 1;
-        dep_window<ORDER, R, MODE, SY, SZ, V>(Js, EX, EY, EZ, wq * qdx * scx, wq * qdy * scy,
-                                              wq * qdz * scz);
-      }
-    };
-    // Rounds of blockDim particles.  In a hot tile the queue is drained
-    // between rounds (a block-uniform point) whenever the next round might
-    // not fit, so node-changing particles never take the divergent in-line
-    // path; other tiles run barrier-free and drain once at the end.
-    for (int base = pbeg; base < pend; base += blockDim.x) {
-     const int ip = base + threadIdx.x;
-     if (ip < pend) {
+    for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
       int ci, cj, ck;
       unpack_cell(cellp[ip], ci, cj, ck);
       const R ox = oxp[ip], oy = oyp[ip], oz = ozp[ip];
@@ -769,16 +709,11 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
           if (!ok) bad = 1;
           if (in_new) {
             const int q = atomicAdd(&s_qn, 1);
-            if (q < QC) {
-              q_ip[q] = ip;
-              q_pk[q] = (unsigned)(vx + D + L) | ((unsigned)(vy + D + L) << 8) |
-                        ((unsigned)(vz + D + L) << 16) | ((unsigned)(sx + 1) << 24) |
-                        ((unsigned)(sy + 1) << 26) | ((unsigned)(sz + 1) << 28);
-              q_o[q] = ox; q_o[QC + q] = oy; q_o[2 * QC + q] = oz;
-            } else {
-              dep_window_general<ORDER, R, MODE, SY, SZ, V>(Js, EX, EY, EZ, wq * qdx * scx,
-                                                            wq * qdy * scy, wq * qdz * scz);
-            }
+            q_list[pbeg + q] = ip;
+            q_pk[ip] = (unsigned)(vx + D + L) | ((unsigned)(vy + D + L) << 8) |
+                       ((unsigned)(vz + D + L) << 16) | ((unsigned)(sx + 1) << 24) |
+                       ((unsigned)(sy + 1) << 26) | ((unsigned)(sz + 1) << 28);
+            q_ox[ip] = ox; q_oy[ip] = oy; q_oz[ip] = oz;
           } else {
             ++nslow;
             dep_global<ORDER, R>(sj, EX, EY, EZ, wq * qdx, wq * qdy, wq * qdz);
@@ -795,20 +730,33 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       uxp[ip] = ux; uyp[ip] = uy; uzp[ip] = uz;
       const double u2 = (double)ux * ux + (double)uy * uy + (double)uz * uz;
       ke += u2 * c2i / (1.0 + sqrt(1.0 + u2 * c2i)) * (double)wgt;
-     }
-      if (hot && base + (int)blockDim.x < pend) {
-        __syncthreads();
-        if (s_qn + (int)blockDim.x > QC) {
-          flush_queue();
-          __syncthreads();
-          if (threadIdx.x == 0) s_qn = 0;
-          __syncthreads();
-        }
-      }
     }
     __syncthreads();
-    // ---- remaining queued window particles with a node change ---------------
-    flush_queue();
+    // ---- deferred window particles with a node change ------------------------
+    {
+      const int nq = s_qn;
+      for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const int ip = q_list[pbeg + q];
+        const unsigned pk = q_pk[ip];
+        const int bx = pk & 255u, by = (pk >> 8) & 255u, bz = (pk >> 16) & 255u;
+        const int sx = (int)((pk >> 24) & 3u) - 1, sy = (int)((pk >> 26) & 3u) - 1,
+                  sz = (int)((pk >> 28) & 3u) - 1;
+        const R ox = q_ox[ip], oy = q_oy[ip], oz = q_oz[ip];
+        const R nox = oxp[ip], noy = oyp[ip], noz = ozp[ip], wq = wp[ip];
+        int r0, r1;
+        R a0, a1;
+        EsirAxis<ORDER, R> EX, EY, EZ;
+        esir_node<ORDER, R>(nox, r0, a0); esir_node<ORDER, R>(ox, r1, a1);
+        bool ok = EX.set(bx + sx + r0, a0, bx + r1, a1);
+        esir_node<ORDER, R>(noy, r0, a0); esir_node<ORDER, R>(oy, r1, a1);
+        ok = EY.set(by + sy + r0, a0, by + r1, a1) && ok;
+        esir_node<ORDER, R>(noz, r0, a0); esir_node<ORDER, R>(oz, r1, a1);
+        ok = EZ.set(bz + sz + r0, a0, bz + r1, a1) && ok;
+        if (!ok) bad = 1;
+        dep_window<ORDER, R, MODE, SY, SZ, V>(Js, EX, EY, EZ, wq * qdx * scx, wq * qdy * scy,
+                                              wq * qdz * scz);
+      }
+    }
     __syncthreads();
     // ---- flush the J window: FP64 atomics into the periodic grid -------------
     {
