@@ -463,9 +463,14 @@ def run_accuracy(wl, args, pusher, cfg):
     steps = args.accuracy_steps
     sims, one = {}, {}
     t0 = time.perf_counter()
+    from picsar_b200.tiled import SUPPORTED_SHAPES_FP64
+    cfg64 = cfg
+    if (cfg.tile[0], cfg.drift) not in SUPPORTED_SHAPES_FP64:
+        cfg64 = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval,
+                            drift=min(cfg.drift, 1), threads=cfg.threads)
     for prec in ("fp64", "fp32"):
-        t = TiledSim(wl["n"], order=wl["order"], pusher=pusher, precision=prec, config=cfg,
-                     track_ids=True)
+        t = TiledSim(wl["n"], order=wl["order"], pusher=pusher, precision=prec,
+                     config=cfg64 if prec == "fp64" else cfg, track_ids=True)
         t.load_state(st)
         g0 = t.diagnostics(gauss=True)["gauss_norm"]
         t.step(1)

@@ -76,6 +76,8 @@ def _check_layout():
 _I32MAX = 2 ** 31 - 1
 # (tile edge, window margin) pairs the particle kernel is compiled for
 SUPPORTED_SHAPES = {(8, 1), (8, 0), (8, 2), (4, 1), (4, 0)}
+# ... and those of the FP64 engine
+SUPPORTED_SHAPES_FP64 = {(8, 1), (8, 0), (4, 1), (4, 0)}
 # accumulator modes compiled for the FP32 engine per shape (FP64 engine: mode 3)
 SUPPORTED_ACC = {(8, 1): (0, 1, 2), (8, 2): (1, 2), (4, 1): (1, 2)}
 
@@ -123,6 +125,9 @@ class TiledSim:
         if not (tile[0] == tile[1] == tile[2]) or (tile[0], cfg.drift) not in SUPPORTED_SHAPES:
             raise ValueError(f"tile {tile} with drift {cfg.drift} not compiled; "
                              f"supported (edge, drift): {sorted(SUPPORTED_SHAPES)}")
+        if self.prec == 1 and (tile[0], cfg.drift) not in SUPPORTED_SHAPES_FP64:
+            raise ValueError(f"tile {tile} with drift {cfg.drift} not compiled for FP64; "
+                             f"supported (edge, drift): {sorted(SUPPORTED_SHAPES_FP64)}")
         self.tile = tile
         self.g = max(3, cfg.drift + 2)
         if min(self.n) < 2 * self.g:
