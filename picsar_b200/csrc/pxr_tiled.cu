@@ -675,7 +675,7 @@ int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, voi
   cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemsetAsync(J.tile_cnt, 0, sizeof(int32_t) * (ntiles + 1), s) != cudaSuccess)
     return PXRB_ELAUNCH;
-  if (J.tx != J.ty || J.ty != J.tz || J.tx * J.tx * J.tx > RR_MAXC || !J.cell_cnt || !J.rank_b)
+  if (J.tx != J.ty || J.ty != J.tz || J.tx * J.tx * J.tx > RR_MAXC || !J.cell_cnt || (J.np > 0 && !J.rank_b))
     return PXRB_EINVAL;
   if (cudaMemsetAsync(J.cell_cnt, 0, sizeof(int32_t) * (size_t)ntiles * J.tx * J.tx * J.tx, s) !=
       cudaSuccess)
