@@ -222,6 +222,7 @@ typedef struct pxrb_tiled_job {
                                                [1] error flag */
   int32_t* cell_cnt;                        /* sort scratch: ntiles * tile^3 */
   int32_t* rank_b;                          /* sort scratch: np */
+  int32_t* perm;                            /* sort scratch: np */
 } pxrb_tiled_job;
 
 /* Tile shapes: cubic tiles of edge tx = ty = tz = `tile` in {4, 8} with window
@@ -284,14 +285,14 @@ int pxrb_tiled_push_e(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t pre
  * distinct shared-memory banks of the tile window: a warp of the particle
  * kernel then touches 32 different cells without bank conflicts.  Rebuilds
  * tile_off; the particle arrays keep their addresses (the *_b buffers, and
- * cell_cnt / rank_b, are scratch).  job_host: host copy (sizes and pointers);
+ * cell_cnt / rank_b / perm, are scratch).  job_host: host copy (sizes and pointers);
  * job_dev: the device copy the kernels read. */
 int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, void* stream);
 
 /* The same sort for a batch of jobs in five launches (an ensemble, the
  * reference's per-species pxr_particle_sorting over many simulations).
  * jobs_dev: DEVICE array of njobs descriptors, all of precision `prec`, each
- * with cubic tiles of edge <= 8 and cell_cnt / rank_b set; max_tiles: at
+ * with cubic tiles of edge 4 or 8 and cell_cnt / rank_b / perm set; max_tiles: at
  * least the tile count of every job; max_np: the largest particle count
  * (sizes the grid only).  The counters are cleared on the device, so the
  * call needs no host copy of the descriptors. */

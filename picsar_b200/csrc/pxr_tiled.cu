@@ -185,12 +185,30 @@ __global__ void __launch_bounds__(YEE_TPB)
 }
 
 // ---------------------------------------------------------------------------
-// Counting sort by tile.
+// Counting sort by tile (cubic tiles, edge 4 or 8).
+//   count:    per particle, its rank inside its cell (atomic on the cell's
+//             counter, kept in rank_b);
+//   cellscan: per tile, cell counts -> exclusive prefixes in place (cell_cnt)
+//             and the tile total (tile_cnt);
+//   scan:     tile totals -> tile_off;
+//   perm:     perm[tile_off + prefix(cell) + rank] = p (cell-major order
+//             inside the tile; only a 4-byte index moves);
+//   rr:       per tile, walks its round-robin destinations in order, finds
+//             each one's (cell, rank) and source p through perm, and gathers
+//             the particle into the *_b buffers (coalesced writes);
+//   copy:     *_b -> primary arrays (coalesced).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int tile_of(const Job& J, uint32_t cell) {
+struct TileCell {
+  int t, lc;
+};
+__device__ __forceinline__ TileCell tile_cell(const Job& J, uint32_t cell) {
   int i, j, k;
   unpack_cell(cell, i, j, k);
-  return i / J.tx + J.ntx * (j / J.ty + J.nty * (k / J.tz));
+  const int sh = __ffs(J.tx) - 1, m = J.tx - 1;      // power-of-two edge
+  TileCell r;
+  r.t = (i >> sh) + J.ntx * ((j >> sh) + J.nty * (k >> sh));
+  r.lc = (i & m) + J.tx * ((j & m) + J.tx * (k & m));
+  return r;
 }
 
 // Clears the tile counters and per-cell counters of every job of a batch
@@ -207,23 +225,56 @@ __global__ void k_sort_zero(const Job* __restrict__ jp) {
 }
 
 __global__ void k_sort_count(const Job* __restrict__ jp) {
+  const Job J = jp[blockIdx.y];            // by value: fields stay in registers
+  const int T3 = J.tx * J.tx * J.tx;
+  const uint32_t* __restrict__ cell = J.cell;
+  int* __restrict__ rank = J.rank_b;
+  int* __restrict__ cc = J.cell_cnt;
+  const i64 np = J.np;
+  for (i64 p = blockIdx.x * (i64)blockDim.x + threadIdx.x; p < np;
+       p += (i64)gridDim.x * blockDim.x) {
+    const TileCell tc = tile_cell(J, cell[p]);
+    rank[p] = atomicAdd(&cc[(i64)tc.t * T3 + tc.lc], 1);
+  }
+}
+
+// One warp per tile: exclusive prefix of the tile's cell counts, in place,
+// and the tile total.
+constexpr int CS_TPB = 256;
+__global__ void __launch_bounds__(CS_TPB) k_sort_cellscan(const Job* __restrict__ jp) {
   const Job& J = jp[blockIdx.y];
   const int ntiles = J.ntx * J.nty * J.ntz;
-  for (i64 p = blockIdx.x * (i64)blockDim.x + threadIdx.x; p < J.np;
-       p += (i64)gridDim.x * blockDim.x) {
-    int t = tile_of(J, J.cell[p]);
-    // aggregate equal tiles inside the warp
-    unsigned mask = __activemask();
-    unsigned peers = __match_any_sync(mask, t);
-    int leader = __ffs(peers) - 1;
-    if ((threadIdx.x & 31) == leader) atomicAdd(&J.tile_cnt[t], __popc(peers));
-    (void)ntiles;
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x * (CS_TPB / 32) + (threadIdx.x >> 5);
+  if (t >= ntiles) return;
+  const int T3 = J.tx * J.tx * J.tx, per = (T3 + 31) / 32;
+  int* c = J.cell_cnt + (i64)t * T3;
+  int v[16];
+  int sum = 0;
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int lc = lane * per + u;
+    v[u] = (u < per && lc < T3) ? c[lc] : 0;
+    sum += v[u];
   }
+  int incl = sum;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += y;
+  }
+  int run = incl - sum;
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int lc = lane * per + u;
+    if (u < per && lc < T3) { c[lc] = run; run += v[u]; }
+  }
+  if (lane == 31) J.tile_cnt[t] = incl;
 }
 
 constexpr int SCAN_TPB = 1024;
 
-// exclusive scan of tile_cnt into tile_off, cursor copy left in tile_cnt
+// exclusive scan of tile_cnt into tile_off
 __global__ void __launch_bounds__(SCAN_TPB) k_sort_scan(const Job* __restrict__ jp) {
   typedef cub::BlockScan<int, SCAN_TPB> Scan;
   __shared__ typename Scan::TempStorage tmp;
@@ -238,7 +289,7 @@ __global__ void __launch_bounds__(SCAN_TPB) k_sort_scan(const Job* __restrict__ 
     int ex, tot;
     Scan(tmp).ExclusiveSum(v, ex, tot);
     int c0 = carry;
-    if (t < ntiles) { J.tile_off[t] = c0 + ex; J.tile_cnt[t] = c0 + ex; }
+    if (t < ntiles) J.tile_off[t] = c0 + ex;
     __syncthreads();
     if (threadIdx.x == 0) carry = c0 + tot;
     __syncthreads();
@@ -246,51 +297,75 @@ __global__ void __launch_bounds__(SCAN_TPB) k_sort_scan(const Job* __restrict__ 
   if (threadIdx.x == 0) J.tile_off[ntiles] = carry;
 }
 
-template <typename R>
-__global__ void k_sort_scatter(const Job* __restrict__ jp) {
-  const Job& J = jp[blockIdx.y];
-  const R *ox = (const R*)J.ox, *oy = (const R*)J.oy, *oz = (const R*)J.oz;
-  const R *ux = (const R*)J.ux, *uy = (const R*)J.uy, *uz = (const R*)J.uz, *w = (const R*)J.w;
-  R *ox2 = (R*)J.ox_b, *oy2 = (R*)J.oy_b, *oz2 = (R*)J.oz_b;
-  R *ux2 = (R*)J.ux_b, *uy2 = (R*)J.uy_b, *uz2 = (R*)J.uz_b, *w2 = (R*)J.w_b;
-  for (i64 p = blockIdx.x * (i64)blockDim.x + threadIdx.x; p < J.np;
+__global__ void k_sort_perm(const Job* __restrict__ jp) {
+  const Job J = jp[blockIdx.y];
+  const int T3 = J.tx * J.tx * J.tx;
+  const uint32_t* __restrict__ cell = J.cell;
+  const int* __restrict__ rank = J.rank_b;
+  const int* __restrict__ cc = J.cell_cnt;
+  const int* __restrict__ toff = J.tile_off;
+  int* __restrict__ perm = J.perm;
+  const i64 np = J.np;
+  for (i64 p = blockIdx.x * (i64)blockDim.x + threadIdx.x; p < np;
        p += (i64)gridDim.x * blockDim.x) {
-    uint32_t cell = J.cell[p];
-    int t = tile_of(J, cell);
-    unsigned mask = __activemask();
-    unsigned peers = __match_any_sync(mask, t);
-    int lane = threadIdx.x & 31;
-    int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(&J.tile_cnt[t], __popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    int slot = base + __popc(peers & ((1u << lane) - 1u));
-    // rank of the particle inside its cell
-    {
-      int ci, cj, ck;
-      unpack_cell(cell, ci, cj, ck);
-      const int T = J.tx;
-      const int lc = (ci % T) + T * ((cj % T) + T * (ck % T));
-      const unsigned cpeers = __match_any_sync(mask, cell);
-      const int cl = __ffs(cpeers) - 1;
-      int cbase = 0;
-      if (lane == cl) cbase = atomicAdd(&J.cell_cnt[(i64)t * T * T * T + lc], __popc(cpeers));
-      cbase = __shfl_sync(cpeers, cbase, cl);
-      J.rank_b[slot] = cbase + __popc(cpeers & ((1u << lane) - 1u));
-    }
-    J.cell_b[slot] = cell;
-    ox2[slot] = ox[p]; oy2[slot] = oy[p]; oz2[slot] = oz[p];
-    ux2[slot] = ux[p]; uy2[slot] = uy[p]; uz2[slot] = uz[p]; w2[slot] = w[p];
-    if (J.pid) J.pid_b[slot] = J.pid[p];
+    const TileCell tc = tile_cell(J, cell[p]);
+    perm[toff[tc.t] + cc[(i64)tc.t * T3 + tc.lc] + rank[p]] = (int)p;
   }
 }
 
+// One array per blockIdx.z (cell, 7 reals, pid): a plain coalesced copy.
+template <typename R>
+__global__ void k_sort_copy(const Job* __restrict__ jp) {
+  const Job J = jp[blockIdx.y];
+  const i64 np = J.np;
+  const int a = blockIdx.z;
+  const void* src;
+  void* dst;
+  int es = sizeof(R);
+  switch (a) {
+    case 0: src = J.cell_b; dst = J.cell; es = 4; break;
+    case 1: src = J.ox_b; dst = J.ox; break;
+    case 2: src = J.oy_b; dst = J.oy; break;
+    case 3: src = J.oz_b; dst = J.oz; break;
+    case 4: src = J.ux_b; dst = J.ux; break;
+    case 5: src = J.uy_b; dst = J.uy; break;
+    case 6: src = J.uz_b; dst = J.uz; break;
+    case 7: src = J.w_b; dst = J.w; break;
+    default: src = J.pid_b; dst = J.pid; es = 4; break;
+  }
+  if (!src || !dst) return;
+  // 16-byte chunks (torch allocations are 256-byte aligned), then the tail
+  const i64 bytes = np * es, n16 = bytes / 16;
+  const uint4* __restrict__ s4 = (const uint4*)src;
+  uint4* __restrict__ d4 = (uint4*)dst;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n16;
+       i += (i64)gridDim.x * blockDim.x)
+    d4[i] = __ldg(s4 + i);
+  const i64 tail = bytes - n16 * 16;
+  if (blockIdx.x == 0 && threadIdx.x < tail)
+    ((unsigned char*)dst)[n16 * 16 + threadIdx.x] = ((const unsigned char*)src)[n16 * 16 + threadIdx.x];
+}
 
-// Round-robin layout of one tile (one CTA per tile): particles come tile-
-// sorted from the *_b buffers with their rank inside their cell; position =
-// (all particles of lower rank) + (cells of this rank earlier in the bank
-// order).  The bank order lists cells by (g, rho): rho = window address of the
-// cell mod 32, g = index of the cell among those with the same rho.
+// position of the k-th (0-based) set bit of m
+__device__ __forceinline__ int select_bit(unsigned m, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const unsigned low = (1u << w) - 1u;
+    const int c = __popc(m & low);
+    if (k >= c) { k -= c; m >>= w; pos += w; } else { m &= low; }
+  }
+  return pos;
+}
+
+// Round-robin layout of one tile (one CTA per tile): the tile's particles
+// come cell-major from the *_b buffers (scatter), so a particle's cell and
+// its rank inside the cell follow from its position and the cell prefixes.
+// Final position = (all particles of lower rank) + (cells of this rank
+// earlier in the bank order).  The bank order lists cells by (g, rho): rho =
+// window address of the cell mod 32, g = index of the cell among those with
+// the same rho, so 32 consecutive particles of one rank sit in cells whose
+// shared-memory window addresses fall in distinct banks.
 constexpr int RR_TPB = 256;
 constexpr int RR_MAXR = 64;      // ranks handled per pass
 constexpr int RR_MAXC = 512;     // cells per tile (tile edge <= 8)
@@ -303,56 +378,93 @@ __global__ void __launch_bounds__(RR_TPB) k_sort_rr(const Job* __restrict__ jp) 
   if (t >= J.ntx * J.nty * J.ntz) return;
   const int b0 = J.tile_off[t], b1 = J.tile_off[t + 1];
   if (b0 == b1) return;
-  __shared__ int cnt[RR_MAXC], key[RR_MAXC], pos_of[RR_MAXC], cell_at[RR_MAXC];
+  __shared__ int pre[RR_MAXC], cnt[RR_MAXC], key[RR_MAXC], pos_of[RR_MAXC], cell_at[RR_MAXC];
+  __shared__ int chunk[RR_MAXC / 32][32];
+  __shared__ int tot[32];
   __shared__ unsigned bits[RR_MAXR][RR_MAXC / 32];
   __shared__ int wpre[RR_MAXR][RR_MAXC / 32 + 1];
-  __shared__ int base_r[RR_MAXR];
+  __shared__ int base_r[RR_MAXR + 1];
   __shared__ int s_maxr, s_carry;
   const int L = J.order == 1 ? 0 : 1, H = J.order == 1 ? 1 : 2;
   const int W = T + 2 * J.drift + L + H;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int nchunk = (T3 + 31) / 32;
   if (threadIdx.x == 0) { s_maxr = 0; s_carry = 0; }
+  for (int e = threadIdx.x; e < nchunk * 32; e += blockDim.x) chunk[e / 32][e % 32] = 0;
   for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
-    cnt[lc] = J.cell_cnt[(i64)t * T3 + lc];
+    pre[lc] = J.cell_cnt[(i64)t * T3 + lc];
     const int x = lc % T, y = (lc / T) % T, z = lc / (T * T);
-    key[lc] = (x + W * y + W * W * z) & 31;          // residue for now
+    key[lc] = (x + W * y + W * W * z) & 31;          // residue rho
   }
   __syncthreads();
+  // g = rank of the cell among earlier cells with the same residue: inside
+  // each 32-cell chunk by warp matching, across chunks by per-residue prefix
+  for (int c = wid; c < nchunk; c += nwarp) {
+    const int lc = c * 32 + lane;
+    const int r = lc < T3 ? key[lc] : 32 + lane;      // distinct dummies past the end
+    const unsigned peers = __match_any_sync(0xffffffffu, r);
+    if (lc < T3) {
+      pos_of[lc] = __popc(peers & ((1u << lane) - 1u));     // rank inside the chunk
+      if (lane == __ffs(peers) - 1) chunk[c][r] = __popc(peers);
+    }
+  }
   for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
-    const int rho = key[lc];
-    int g = 0;
-    for (int c = 0; c < lc; ++c) g += (key[c] == rho);
-    pos_of[lc] = g * 32 + rho;                        // final key, stored aside
+    const int hi = lc + 1 < T3 ? pre[lc + 1] : b1 - b0;
+    cnt[lc] = hi - pre[lc];
     atomicMax(&s_maxr, cnt[lc]);
   }
   __syncthreads();
-  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) key[lc] = pos_of[lc];
+  if (threadIdx.x < 32) {
+    int acc = 0;
+    for (int c = 0; c < nchunk; ++c) { const int v = chunk[c][threadIdx.x]; chunk[c][threadIdx.x] = acc; acc += v; }
+    tot[threadIdx.x] = acc;
+  }
+  __syncthreads();
+  // position of key (g, rho) in the bank order: cells with a lower g, plus
+  // cells with the same g and a lower rho
+  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
+    const int rho = key[lc];
+    const int g = chunk[lc / 32][rho] + pos_of[lc];
+    int q = 0;
+#pragma unroll 8
+    for (int r2 = 0; r2 < 32; ++r2) {
+      const int n2 = tot[r2];
+      q += min(n2, g) + ((r2 < rho && n2 > g) ? 1 : 0);
+    }
+    key[lc] = q;                                      // reuse: bank-order index
+  }
   __syncthreads();
   for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
-    const int k = key[lc];
-    int q = 0;
-    for (int c = 0; c < T3; ++c) q += (key[c] < k);
-    pos_of[lc] = q;
-    cell_at[q] = lc;
+    pos_of[lc] = key[lc];
+    cell_at[key[lc]] = lc;
   }
   __syncthreads();
   const int nw = (T3 + 31) / 32;
   const int maxr = s_maxr;
-  const R *ox = (const R*)J.ox_b, *oy = (const R*)J.oy_b, *oz = (const R*)J.oz_b;
-  const R *ux = (const R*)J.ux_b, *uy = (const R*)J.uy_b, *uz = (const R*)J.uz_b;
-  const R* w = (const R*)J.w_b;
-  R *ox2 = (R*)J.ox, *oy2 = (R*)J.oy, *oz2 = (R*)J.oz;
-  R *ux2 = (R*)J.ux, *uy2 = (R*)J.uy, *uz2 = (R*)J.uz, *w2 = (R*)J.w;
-  const int ti = t % J.ntx, tj = (t / J.ntx) % J.nty, tk = t / (J.ntx * J.nty);
+  const R* __restrict__ ox = (const R*)J.ox;
+  const R* __restrict__ oy = (const R*)J.oy;
+  const R* __restrict__ oz = (const R*)J.oz;
+  const R* __restrict__ ux = (const R*)J.ux;
+  const R* __restrict__ uy = (const R*)J.uy;
+  const R* __restrict__ uz = (const R*)J.uz;
+  const R* __restrict__ w = (const R*)J.w;
+  R *ox2 = (R*)J.ox_b, *oy2 = (R*)J.oy_b, *oz2 = (R*)J.oz_b;
+  R *ux2 = (R*)J.ux_b, *uy2 = (R*)J.uy_b, *uz2 = (R*)J.uz_b, *w2 = (R*)J.w_b;
+  const int* __restrict__ perm = J.perm;
+  const uint32_t* __restrict__ cell_src = J.cell;
+  uint32_t* __restrict__ cell_dst = J.cell_b;
+  const int* __restrict__ pid_src = J.pid;
+  int* __restrict__ pid_dst = J.pid_b;
   for (int r0 = 0; r0 < maxr; r0 += RR_MAXR) {
     const int nr = min(RR_MAXR, maxr - r0);
     for (int e = threadIdx.x; e < nr * nw; e += blockDim.x) {
       const int i = e / nw, wd = e % nw;
-      unsigned m = 0;
+      unsigned mk = 0;
       for (int b = 0; b < 32; ++b) {
         const int q = wd * 32 + b;
-        if (q < T3 && cnt[cell_at[q]] > r0 + i) m |= 1u << b;
+        if (q < T3 && cnt[cell_at[q]] > r0 + i) mk |= 1u << b;
       }
-      bits[i][wd] = m;
+      bits[i][wd] = mk;
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nr; i += blockDim.x) {
@@ -364,23 +476,33 @@ __global__ void __launch_bounds__(RR_TPB) k_sort_rr(const Job* __restrict__ jp) 
     if (threadIdx.x == 0) {
       int c = s_carry;
       for (int i = 0; i < nr; ++i) { base_r[i] = c; c += wpre[i][nw]; }
+      base_r[nr] = c;          // end of this pass's destinations
       s_carry = c;
     }
     __syncthreads();
-    for (int p = b0 + threadIdx.x; p < b1; p += blockDim.x) {
-      const int r = J.rank_b[p];
-      if (r < r0 || r >= r0 + nr) continue;
-      const uint32_t cell = J.cell_b[p];
-      int ci, cj, ck;
-      unpack_cell(cell, ci, cj, ck);
-      const int lc = (ci - ti * T) + T * ((cj - tj * T) + T * (ck - tk * T));
-      const int q = pos_of[lc], i = r - r0;
-      const int pos = base_r[i] + wpre[i][q >> 5] + __popc(bits[i][q >> 5] & ((1u << (q & 31)) - 1u));
-      const int d = b0 + pos;
-      J.cell[d] = cell;
-      ox2[d] = ox[p]; oy2[d] = oy[p]; oz2[d] = oz[p];
-      ux2[d] = ux[p]; uy2[d] = uy[p]; uz2[d] = uz[p]; w2[d] = w[p];
-      if (J.pid) J.pid[d] = J.pid_b[p];
+    // destinations of this pass, in order: d -> rank i (binary search over
+    // the blocks), k-th cell of that rank in bank order (word prefix, then
+    // bit select), source through perm (cell-major slot)
+    const int dbeg = base_r[0], dend = base_r[nr];
+    for (int o = dbeg + threadIdx.x; o < dend; o += blockDim.x) {
+      int lo = 0, hi = nr - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (base_r[mid] <= o) lo = mid; else hi = mid - 1;
+      }
+      const int i = lo;
+      int k = o - base_r[i];
+      int wd = 0;
+      while (wd + 1 < nw && wpre[i][wd + 1] <= k) ++wd;
+      const int q = wd * 32 + select_bit(bits[i][wd], k - wpre[i][wd]);
+      const int lc = cell_at[q];
+      const int p = perm[b0 + pre[lc] + r0 + i];
+      const int d = b0 + o;
+      cell_dst[d] = __ldg(cell_src + p);
+      ox2[d] = __ldg(ox + p); oy2[d] = __ldg(oy + p); oz2[d] = __ldg(oz + p);
+      ux2[d] = __ldg(ux + p); uy2[d] = __ldg(uy + p); uz2[d] = __ldg(uz + p);
+      w2[d] = __ldg(w + p);
+      if (pid_src) pid_dst[d] = __ldg(pid_src + p);
     }
     __syncthreads();
   }
@@ -680,16 +802,22 @@ int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, voi
   if (cudaMemsetAsync(J.cell_cnt, 0, sizeof(int32_t) * (size_t)ntiles * J.tx * J.tx * J.tx, s) !=
       cudaSuccess)
     return PXRB_ELAUNCH;
+  if (J.tx != 4 && J.tx != 8) return PXRB_EUNSUPPORTED;
   const int nb = gs_blocks(J.np, 256);
-  if (J.np > 0) k_sort_count<<<nb, 256, 0, s>>>(job_dev);
+  if (J.np > 0) {
+    k_sort_count<<<nb, 256, 0, s>>>(job_dev);
+    k_sort_cellscan<<<(ntiles + CS_TPB / 32 - 1) / (CS_TPB / 32), CS_TPB, 0, s>>>(job_dev);
+  }
   k_sort_scan<<<1, SCAN_TPB, 0, s>>>(job_dev);
   if (J.np > 0) {
+    if (!J.perm) return PXRB_EINVAL;
+    k_sort_perm<<<nb, 256, 0, s>>>(job_dev);
     if (J.prec == 0) {
-      k_sort_scatter<float><<<nb, 256, 0, s>>>(job_dev);
       k_sort_rr<float><<<ntiles, RR_TPB, 0, s>>>(job_dev);
+      k_sort_copy<float><<<dim3(nb, 1, 9), 256, 0, s>>>(job_dev);
     } else {
-      k_sort_scatter<double><<<nb, 256, 0, s>>>(job_dev);
       k_sort_rr<double><<<ntiles, RR_TPB, 0, s>>>(job_dev);
+      k_sort_copy<double><<<dim3(nb, 1, 9), 256, 0, s>>>(job_dev);
     }
   }
   PXRB_CHECK_LAUNCH();
@@ -708,15 +836,18 @@ int pxrb_tiled_sort_batch(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t
   const int cap = njobs >= 4096 ? 1 : 4096 / njobs;
   const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
   const dim3 g_np(bx, njobs), g_one(1, njobs), g_tiles(max_tiles, njobs);
+  const dim3 g_cs((max_tiles + CS_TPB / 32 - 1) / (CS_TPB / 32), njobs);
   k_sort_zero<<<g_np, 256, 0, s>>>(jobs_dev);
   k_sort_count<<<g_np, 256, 0, s>>>(jobs_dev);
+  k_sort_cellscan<<<g_cs, CS_TPB, 0, s>>>(jobs_dev);
   k_sort_scan<<<g_one, SCAN_TPB, 0, s>>>(jobs_dev);
+  k_sort_perm<<<g_np, 256, 0, s>>>(jobs_dev);
   if (prec == 0) {
-    k_sort_scatter<float><<<g_np, 256, 0, s>>>(jobs_dev);
     k_sort_rr<float><<<g_tiles, RR_TPB, 0, s>>>(jobs_dev);
+    k_sort_copy<float><<<dim3(g_np.x, njobs, 9), 256, 0, s>>>(jobs_dev);
   } else {
-    k_sort_scatter<double><<<g_np, 256, 0, s>>>(jobs_dev);
     k_sort_rr<double><<<g_tiles, RR_TPB, 0, s>>>(jobs_dev);
+    k_sort_copy<double><<<dim3(g_np.x, njobs, 9), 256, 0, s>>>(jobs_dev);
   }
   PXRB_CHECK_LAUNCH();
   return PXRB_OK;

@@ -97,7 +97,7 @@ def job_bytes(spec: JobSpec, precision="fp32", config: TiledConfig | None = None
     fcells = pitch * (nt[1] * t + 2 * g) * (nt[2] * t + 2 * g)
     ntiles = nt[0] * nt[1] * nt[2]
     grid = 6 * fcells * r + 4 * spec.cells * 8 + ntiles * (t ** 3 * 4 + 16)
-    parts = spec.particles * (2 * (7 * r + 4) + 4)
+    parts = spec.particles * (2 * (7 * r + 4) + 8)
     return int(grid + parts + (1 << 16))
 
 
@@ -274,7 +274,7 @@ class Ensemble:
                             g.replay()
                     else:
                         self._launch_sort(grp)
-                    self.launches += 5
+                    self.launches += 7
 
     # ------------------------------------------------------------ results
     def sims(self):
@@ -325,7 +325,7 @@ class Ensemble:
                 K = grp.cfg.sort_interval
                 if K > 0 and self.it % K == 0:
                     self._launch_sort(grp)
-                    self.launches += 5
+                    self.launches += 7
             torch.cuda.synchronize()
             pk += ev[0].elapsed_time(ev[1])
             yee += ev[1].elapsed_time(ev[2])

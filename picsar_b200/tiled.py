@@ -41,7 +41,7 @@ class TiledJob(C.Structure):
         + [(n, _P) for n in ("ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz", "cell", "ox",
                              "oy", "oz", "ux", "uy", "uz", "w", "cell_b", "ox_b", "oy_b", "oz_b",
                              "ux_b", "uy_b", "uz_b", "w_b", "pid", "pid_b", "tile_off",
-                             "tile_cnt", "ke_tile", "counters", "cell_cnt", "rank_b")]
+                             "tile_cnt", "ke_tile", "counters", "cell_cnt", "rank_b", "perm")]
     )
 
 
@@ -224,10 +224,12 @@ class TiledSim:
         self.cell = torch.empty(N, dtype=torch.int32, device=dev)
         self.cell_b = torch.empty(N, dtype=torch.int32, device=dev)
         self.rank_b = torch.empty(N, dtype=torch.int32, device=dev)
+        self.perm = torch.empty(N, dtype=torch.int32, device=dev)
         j = self.job
         j.np = N
         j.cell, j.cell_b = self.cell.data_ptr(), self.cell_b.data_ptr()
         j.rank_b = self.rank_b.data_ptr()
+        j.perm = self.perm.data_ptr()
         for c in ("ox", "oy", "oz", "ux", "uy", "uz", "w"):
             setattr(j, c, self.parts[c].data_ptr())
             setattr(j, c + "_b", self.parts_b[c].data_ptr())
@@ -267,7 +269,7 @@ class TiledSim:
         # sizes, tile_cnt and tile_off of the host descriptor never change;
         # the particle pointers it holds may be stale (the device swaps them)
         _lib.call("pxrb_tiled_sort", self._jp(), self.job_dev.data_ptr(), _stream())
-        self.launches += 4 if self.np > 0 else 1
+        self.launches += 6 if self.np > 0 else 1
 
     def particle_step(self):
         ctas = min(self.ntiles, self.num_sms * self.cfg.ctas_per_sm)
@@ -379,7 +381,7 @@ class TiledSim:
             tot += t.numel() * t.element_size()
         if self.np:
             tot += sum(t.numel() * t.element_size() for t in self.parts.values()) * 2
-            tot += self.cell.numel() * 8
+            tot += self.cell.numel() * 12
         return tot
 
 

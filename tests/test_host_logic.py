@@ -28,8 +28,8 @@ def test_ensemble_distribution():
 def test_job_bytes_scales():
     a = JobSpec(n=(32, 32, 32), ppc=8, sigma=0.01, order=1)
     b = JobSpec(n=(32, 32, 32), ppc=16, sigma=0.01, order=1)
-    # FP32: 7 reals and the packed cell twice (sort buffers) + rank = 68 B/particle
-    assert job_bytes(b, "fp32") - job_bytes(a, "fp32") == 32 ** 3 * 8 * 68
+    # FP32: 7 reals and the packed cell twice (sort buffers) + rank + perm = 72 B/particle
+    assert job_bytes(b, "fp32") - job_bytes(a, "fp32") == 32 ** 3 * 8 * 72
     assert job_bytes(a, "fp64") > job_bytes(a, "fp32")
 
 
