@@ -645,7 +645,7 @@ __global__ void __launch_bounds__(RED_TPB) k_field_sums(Job J, const double* rho
   const int nx = J.nx, ny = J.ny, nz = J.nz, G = J.g, pitch = J.pitch_x, NYg = J.pitch_y;
   const i64 sy = pitch, sz = (i64)pitch * NYg;
   const i64 total = (i64)nx * ny * nz;
-  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   const R* F[6] = {(const R*)J.ex, (const R*)J.ey, (const R*)J.ez,
                    (const R*)J.bx, (const R*)J.by, (const R*)J.bz};
   for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < total;
@@ -666,40 +666,42 @@ __global__ void __launch_bounds__(RED_TPB) k_field_sums(Job J, const double* rho
       acc[7] += r * r;
     }
   }
-  __shared__ double red[8][RED_TPB / 32];
-  for (int q = 0; q < 8; ++q) {
+  {
+    // kinetic energy: this block's fixed slice of the per-tile sums
+    const int ntiles = J.ntx * J.nty * J.ntz;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < ntiles; b += gridDim.x * blockDim.x)
+      acc[8] += J.ke_tile[b];
+  }
+  __shared__ double red[9][RED_TPB / 32];
+  for (int q = 0; q < 9; ++q) {
     double v = acc[q];
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 8) {
+  if (threadIdx.x < 9) {
     double s = 0;
     for (int w = 0; w < RED_TPB / 32; ++w) s += red[threadIdx.x][w];
     part[threadIdx.x * gridDim.x + blockIdx.x] = s;
   }
 }
 
-__global__ void k_diag_final(Job J, const double* part, int nblocks, double* out) {
-  // one warp; fixed order
+// Nine warps, one per quantity, each summing that quantity's block partials
+// in a fixed order (deterministic results).
+__global__ void __launch_bounds__(288) k_diag_final(Job J, const double* part, int nblocks,
+                                                    double* out) {
   __shared__ double s[9];
-  if (threadIdx.x < 8) {
-    double t = 0;
-    for (int b = 0; b < nblocks; ++b) t += part[threadIdx.x * nblocks + b];
-    s[threadIdx.x] = t;
-  }
-  if (threadIdx.x == 8) {
-    double t = 0;
-    const int ntiles = J.ntx * J.nty * J.ntz;
-    for (int b = 0; b < ntiles; ++b) t += J.ke_tile[b];
-    s[8] = t;
-  }
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double t = 0;
+  for (int b = lane; b < nblocks; b += 32) t += part[q * nblocks + b];
+  for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+  if (lane == 0) s[q] = t;
   __syncthreads();
   if (threadIdx.x == 0) {
     const double dv = J.dx * J.dy * J.dz;
     out[0] = s[8];
-    for (int q = 0; q < 3; ++q) out[1 + q] = s[q] * dv * J.eps0;
-    for (int q = 3; q < 6; ++q) out[1 + q] = s[q] * dv / J.mu0;
+    for (int c = 0; c < 3; ++c) out[1 + c] = s[c] * dv * J.eps0;
+    for (int c = 3; c < 6; ++c) out[1 + c] = s[c] * dv / J.mu0;
     out[7] = sqrt(s[6]);
     out[8] = sqrt(s[7]);
   }
@@ -908,7 +910,7 @@ int pxrb_tiled_field_export(const pxrb_tiled_job* job_host, int32_t which, doubl
 
 int64_t pxrb_tiled_diag_scratch(const pxrb_tiled_job* job_host) {
   if (!job_host) return -1;
-  return 8 * (int64_t)diag_blocks(*job_host);
+  return 9 * (int64_t)diag_blocks(*job_host);
 }
 
 int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* scratch,
@@ -916,7 +918,7 @@ int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* 
   if (!job_host || !scratch || !out) return PXRB_EINVAL;
   const Job& J = *job_host;
   const int nb = diag_blocks(J);
-  if (scratch_len < 8 * (int64_t)nb) return PXRB_ESCRATCH;
+  if (scratch_len < 9 * (int64_t)nb) return PXRB_ESCRATCH;
   cudaStream_t s = (cudaStream_t)stream;
   if (rho && cudaMemsetAsync(rho, 0, sizeof(double) * (size_t)J.nx * J.ny * J.nz, s) != cudaSuccess)
     return PXRB_ELAUNCH;
@@ -931,7 +933,7 @@ int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* 
   }
   if (J.prec == 0) k_field_sums<float><<<nb, RED_TPB, 0, s>>>(J, rho, scratch);
   else k_field_sums<double><<<nb, RED_TPB, 0, s>>>(J, rho, scratch);
-  k_diag_final<<<1, 32, 0, s>>>(J, scratch, nb, out);
+  k_diag_final<<<1, 288, 0, s>>>(J, scratch, nb, out);
   PXRB_CHECK_LAUNCH();
   return PXRB_OK;
 }
@@ -960,7 +962,7 @@ int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* 
 //    stream capture.
 // ---------------------------------------------------------------------------
 #define PXRB_NOALLOC_RHO_MAX (1 << 20)
-#define PXRB_NOALLOC_PART_MAX (8 * 1184)
+#define PXRB_NOALLOC_PART_MAX (9 * 1184)
 static __device__ __align__(256) double g_noalloc_scratch[PXRB_NOALLOC_RHO_MAX + PXRB_NOALLOC_PART_MAX];
 
 static std::mutex g_noalloc_mu;
@@ -972,7 +974,7 @@ extern "C" int pxrb_tiled_diagnostics_noalloc(const pxrb_tiled_job* job_host, in
   const Job& J = *job_host;
   const i64 ncell = (i64)J.nx * J.ny * J.nz;
   const int nb = diag_blocks(J);
-  if (ncell > PXRB_NOALLOC_RHO_MAX || 8 * nb > PXRB_NOALLOC_PART_MAX) return PXRB_ETOOLARGE;
+  if (ncell > PXRB_NOALLOC_RHO_MAX || 9 * nb > PXRB_NOALLOC_PART_MAX) return PXRB_ETOOLARGE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return PXRB_ELAUNCH;
   double* base = nullptr;

@@ -611,7 +611,6 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     const R clghtisq = (R)(1.0 / (sj.clight * sj.clight));
     const R cst_b = (R)(sj.q * sj.dt * 0.5 / sj.m), cst_v = (R)(sj.q * sj.dt / sj.m);
     const R invc = (R)(1.0 / sj.clight);
-    const double c2i = 1.0 / (sj.clight * sj.clight);
     const R qdx = (R)(sj.q / (sj.dt * sj.dy * sj.dz)), qdy = (R)(sj.q / (sj.dt * sj.dx * sj.dz)),
             qdz = (R)(sj.q / (sj.dt * sj.dx * sj.dy));
     const R scx = (R)scale[0], scy = (R)scale[1], scz = (R)scale[2];
@@ -728,8 +727,12 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       cellp[ip] = pack_cell(nci, ncj, nck);
       oxp[ip] = nox; oyp[ip] = noy; ozp[ip] = noz;
       uxp[ip] = ux; uyp[ip] = uy; uzp[ip] = uz;
-      const double u2 = (double)ux * ux + (double)uy * uy + (double)uz * uz;
-      ke += u2 * c2i / (1.0 + sqrt(1.0 + u2 * c2i)) * (double)wgt;
+      // kinetic energy (gamma - 1) w of the particle in the engine's precision,
+      // summed over the tile in FP64
+      {
+        const R u2 = (ux * ux + uy * uy + uz * uz) * clghtisq;
+        ke += (double)(u2 / ((R)1 + sqrt(u2 + (R)1)) * wgt);
+      }
     }
     __syncthreads();
     // ---- deferred window particles with a node change ------------------------
