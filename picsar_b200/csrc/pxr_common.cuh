@@ -115,14 +115,22 @@ template <int ORDER, typename R> struct StagShape {
 // Boris: src/particle_pushers/boris_pusher/boris_3d.F90:96-131, followed by
 // pxr_set_gamma (:1092-1099).  Vay (which = 0): vay_pusher/vay_3d.F90:100-130.
 // ---------------------------------------------------------------------------
+// 1/sqrt(x) and a/b: correctly rounded in FP64; in FP32 the hardware
+// approximations (rsqrtf, __fdividef: a few ulp), well inside the FP32
+// engine's error budget and several instructions shorter each.
+template <typename R> __device__ __forceinline__ R inv_sqrt(R x) { return (R)1 / sqrt(x); }
+template <> __device__ __forceinline__ float inv_sqrt<float>(float x) { return rsqrtf(x); }
+template <typename R> __device__ __forceinline__ R quot(R a, R b) { return a / b; }
+template <> __device__ __forceinline__ float quot<float>(float a, float b) { return __fdividef(a, b); }
+
 template <typename R>
 __device__ __forceinline__ void boris_push(R& ux, R& uy, R& uz, R& gi, R ex, R ey, R ez,
                                            R bx, R by, R bz, R cst, R clghtisq) {
   ux = ux + ex * cst; uy = uy + ey * cst; uz = uz + ez * cst;
   R usq = (ux * ux + uy * uy + uz * uz) * clghtisq;
-  R gt = (R)1 / sqrt((R)1 + usq);
+  R gt = inv_sqrt<R>((R)1 + usq);
   R tx = gt * bx * cst, ty = gt * by * cst, tz = gt * bz * cst;
-  R tsqi = (R)2 / ((R)1 + tx * tx + ty * ty + tz * tz);
+  R tsqi = quot<R>((R)2, (R)1 + tx * tx + ty * ty + tz * tz);
   R sx = tx * tsqi, sy = ty * tsqi, sz = tz * tsqi;
   R uxp = ux + uy * tz - uz * ty;
   R uyp = uy + uz * tx - ux * tz;
@@ -132,13 +140,13 @@ __device__ __forceinline__ void boris_push(R& ux, R& uy, R& uz, R& gi, R ex, R e
   uz = uz + uxp * sy - uyp * sx;
   ux = ux + ex * cst; uy = uy + ey * cst; uz = uz + ez * cst;
   usq = (ux * ux + uy * uy + uz * uz) * clghtisq;
-  gi = (R)1 / sqrt((R)1 + usq);
+  gi = inv_sqrt<R>((R)1 + usq);
 }
 
 template <typename R>
 __device__ __forceinline__ void set_gamma(R ux, R uy, R uz, R& gi, R clghtisq) {
   R usq = (ux * ux + uy * uy + uz * uz) * clghtisq;
-  gi = (R)1 / sqrt((R)1 + usq);
+  gi = inv_sqrt<R>((R)1 + usq);
 }
 
 // which = 0 full Vay push; const = q dt / m.
@@ -154,11 +162,11 @@ __device__ __forceinline__ void vay_push(R& ux, R& uy, R& uz, R& gi, R ex, R ey,
   R gprsq = ((R)1 + (uxpr * uxpr + uypr * uypr + uzpr * uzpr) * invclightsq);
   R ust = (uxpr * taux + uypr * tauy + uzpr * tauz) * invclight;
   R sigma = gprsq - tausq;
-  R gisq = (R)2 / (sigma + sqrt(sigma * sigma + (R)4 * (tausq + ust * ust)));
+  R gisq = quot<R>((R)2, sigma + sqrt(sigma * sigma + (R)4 * (tausq + ust * ust)));
   gi = sqrt(gisq);
   R bg = bconst * gi;
   R tx = bg * bx, ty = bg * by, tz = bg * bz;
-  R s = (R)1 / ((R)1 + tausq * gisq);
+  R s = quot<R>((R)1, (R)1 + tausq * gisq);
   R tu = tx * uxpr + ty * uypr + tz * uzpr;
   ux = s * (uxpr + tx * tu + uypr * tz - uzpr * ty);
   uy = s * (uypr + ty * tu + uzpr * tx - uxpr * tz);

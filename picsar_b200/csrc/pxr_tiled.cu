@@ -346,101 +346,41 @@ __global__ void k_sort_copy(const Job* __restrict__ jp) {
     ((unsigned char*)dst)[n16 * 16 + threadIdx.x] = ((const unsigned char*)src)[n16 * 16 + threadIdx.x];
 }
 
-// position of the k-th (0-based) set bit of m
-__device__ __forceinline__ int select_bit(unsigned m, int k) {
-  int pos = 0;
-#pragma unroll
-  for (int w = 16; w > 0; w >>= 1) {
-    const unsigned low = (1u << w) - 1u;
-    const int c = __popc(m & low);
-    if (k >= c) { k -= c; m >>= w; pos += w; } else { m &= low; }
-  }
-  return pos;
-}
-
-// Round-robin layout of one tile (one CTA per tile): the tile's particles
-// come cell-major from the *_b buffers (scatter), so a particle's cell and
-// its rank inside the cell follow from its position and the cell prefixes.
-// Final position = (all particles of lower rank) + (cells of this rank
-// earlier in the bank order).  The bank order lists cells by (g, rho): rho =
-// window address of the cell mod 32, g = index of the cell among those with
-// the same rho, so 32 consecutive particles of one rank sit in cells whose
-// shared-memory window addresses fall in distinct banks.
+// Bank-class layout of one tile (one CTA per tile).  The class of a particle
+// is the shared-memory window address of its stencil origin mod 32, i.e. of
+// its cell in the particle kernel's padded window pitch (at order 2 the
+// stencils start at the nearest node, so the cell is shifted by one along
+// each axis where the in-cell offset is >= 1/2).  The tile's particles,
+// taken cell-major, are numbered within their class (level) and laid out by
+// (level, class).  Every 32 consecutive particles then sit in distinct
+// classes, hence distinct banks for every gather load and deposit atomic of
+// a warp, until the smallest class runs out; only the tail beyond it repeats
+// classes, and cell-major numbering keeps those repeats mostly within one
+// cell (one address, a broadcast for the loads).
 constexpr int RR_TPB = 256;
-constexpr int RR_MAXR = 64;      // ranks handled per pass
-constexpr int RR_MAXC = 512;     // cells per tile (tile edge <= 8)
+constexpr int RR_MAXC = 512;        // cells per tile (tile edge <= 8)
+constexpr int RR_LEVELS = 2048;     // level table (larger classes: direct sums)
 
 template <typename R>
 __global__ void __launch_bounds__(RR_TPB) k_sort_rr(const Job* __restrict__ jp) {
   const Job& J = jp[blockIdx.y];
-  const int T = J.tx, T3 = T * T * T;
   const int t = blockIdx.x;
   if (t >= J.ntx * J.nty * J.ntz) return;
   const int b0 = J.tile_off[t], b1 = J.tile_off[t + 1];
   if (b0 == b1) return;
-  __shared__ int pre[RR_MAXC], cnt[RR_MAXC], key[RR_MAXC], pos_of[RR_MAXC], cell_at[RR_MAXC];
-  __shared__ int chunk[RR_MAXC / 32][32];
-  __shared__ int tot[32];
-  __shared__ unsigned bits[RR_MAXR][RR_MAXC / 32];
-  __shared__ int wpre[RR_MAXR][RR_MAXC / 32 + 1];
-  __shared__ int base_r[RR_MAXR + 1];
-  __shared__ int s_maxr, s_carry;
+  __shared__ int s_n[32];                     // class sizes (running)
+  __shared__ int s_w[RR_TPB / 32][32];        // per-warp class counts of a chunk
+  __shared__ int s_P[RR_LEVELS];              // sum_k min(N_k, l)
+  __shared__ unsigned s_M[RR_LEVELS];         // classes k with N_k > l
+  const int T = J.tx;
   const int L = J.order == 1 ? 0 : 1, H = J.order == 1 ? 1 : 2;
   const int W = T + 2 * J.drift + L + H;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  const int nchunk = (T3 + 31) / 32;
-  if (threadIdx.x == 0) { s_maxr = 0; s_carry = 0; }
-  for (int e = threadIdx.x; e < nchunk * 32; e += blockDim.x) chunk[e / 32][e % 32] = 0;
-  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
-    pre[lc] = J.cell_cnt[(i64)t * T3 + lc];
-    const int x = lc % T, y = (lc / T) % T, z = lc / (T * T);
-    key[lc] = (x + W * y + W * W * z) & 31;          // residue rho
-  }
-  __syncthreads();
-  // g = rank of the cell among earlier cells with the same residue: inside
-  // each 32-cell chunk by warp matching, across chunks by per-residue prefix
-  for (int c = wid; c < nchunk; c += nwarp) {
-    const int lc = c * 32 + lane;
-    const int r = lc < T3 ? key[lc] : 32 + lane;      // distinct dummies past the end
-    const unsigned peers = __match_any_sync(0xffffffffu, r);
-    if (lc < T3) {
-      pos_of[lc] = __popc(peers & ((1u << lane) - 1u));     // rank inside the chunk
-      if (lane == __ffs(peers) - 1) chunk[c][r] = __popc(peers);
-    }
-  }
-  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
-    const int hi = lc + 1 < T3 ? pre[lc + 1] : b1 - b0;
-    cnt[lc] = hi - pre[lc];
-    atomicMax(&s_maxr, cnt[lc]);
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    int acc = 0;
-    for (int c = 0; c < nchunk; ++c) { const int v = chunk[c][threadIdx.x]; chunk[c][threadIdx.x] = acc; acc += v; }
-    tot[threadIdx.x] = acc;
-  }
-  __syncthreads();
-  // position of key (g, rho) in the bank order: cells with a lower g, plus
-  // cells with the same g and a lower rho
-  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
-    const int rho = key[lc];
-    const int g = chunk[lc / 32][rho] + pos_of[lc];
-    int q = 0;
-#pragma unroll 8
-    for (int r2 = 0; r2 < 32; ++r2) {
-      const int n2 = tot[r2];
-      q += min(n2, g) + ((r2 < rho && n2 > g) ? 1 : 0);
-    }
-    key[lc] = q;                                      // reuse: bank-order index
-  }
-  __syncthreads();
-  for (int lc = threadIdx.x; lc < T3; lc += blockDim.x) {
-    pos_of[lc] = key[lc];
-    cell_at[key[lc]] = lc;
-  }
-  __syncthreads();
-  const int nw = (T3 + 31) / 32;
-  const int maxr = s_maxr;
+  const int SY = pxrt::win_sy(T, W), SZ = pxrt::win_sz(T, W);
+  const bool half = J.order == 2;
+  const int x0 = (t % J.ntx) * T, y0 = ((t / J.ntx) % J.nty) * T, z0 = (t / (J.ntx * J.nty)) * T;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int* __restrict__ perm = J.perm;
+  const uint32_t* __restrict__ cell = J.cell;
   const R* __restrict__ ox = (const R*)J.ox;
   const R* __restrict__ oy = (const R*)J.oy;
   const R* __restrict__ oz = (const R*)J.oz;
@@ -450,61 +390,87 @@ __global__ void __launch_bounds__(RR_TPB) k_sort_rr(const Job* __restrict__ jp) 
   const R* __restrict__ w = (const R*)J.w;
   R *ox2 = (R*)J.ox_b, *oy2 = (R*)J.oy_b, *oz2 = (R*)J.oz_b;
   R *ux2 = (R*)J.ux_b, *uy2 = (R*)J.uy_b, *uz2 = (R*)J.uz_b, *w2 = (R*)J.w_b;
-  const int* __restrict__ perm = J.perm;
-  const uint32_t* __restrict__ cell_src = J.cell;
-  uint32_t* __restrict__ cell_dst = J.cell_b;
   const int* __restrict__ pid_src = J.pid;
   int* __restrict__ pid_dst = J.pid_b;
-  for (int r0 = 0; r0 < maxr; r0 += RR_MAXR) {
-    const int nr = min(RR_MAXR, maxr - r0);
-    for (int e = threadIdx.x; e < nr * nw; e += blockDim.x) {
-      const int i = e / nw, wd = e % nw;
-      unsigned mk = 0;
-      for (int b = 0; b < 32; ++b) {
-        const int q = wd * 32 + b;
-        if (q < T3 && cnt[cell_at[q]] > r0 + i) mk |= 1u << b;
+  int* lev_at = J.rank_b;                     // level per cell-major slot
+  uint32_t* src_at = J.cell_b;                // source per destination, then its cell
+  auto class_of = [&](int p) {
+    const uint32_t c = __ldg(cell + p);
+    int x = (int)(c & 2047u) - x0, y = (int)((c >> 11) & 2047u) - y0, z = (int)(c >> 22) - z0;
+    if (half) {
+      x += __ldg(ox + p) >= (R)0.5 ? 1 : 0;
+      y += __ldg(oy + p) >= (R)0.5 ? 1 : 0;
+      z += __ldg(oz + p) >= (R)0.5 ? 1 : 0;
+    }
+    return (x + SY * y + SZ * z) & 31;
+  };
+  if (threadIdx.x < 32) s_n[threadIdx.x] = 0;
+  for (int e = threadIdx.x; e < 32 * (RR_TPB / 32); e += blockDim.x) (&s_w[0][0])[e] = 0;
+  __syncthreads();
+  // levels: running per-class counts over cell-major chunks of RR_TPB
+  for (int base = b0; base < b1; base += RR_TPB) {
+    const int sl = base + threadIdx.x;
+    const bool valid = sl < b1;
+    const int k = valid ? class_of(perm[sl]) : 32 + lane;    // distinct dummies
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    const int inw = __popc(peers & ((1u << lane) - 1u));
+    if (valid && lane == __ffs(peers) - 1) s_w[wid][k] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      int lev = s_n[k] + inw;
+      for (int v = 0; v < wid; ++v) lev += s_w[v][k];
+      lev_at[sl] = lev;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      int a = 0;
+      for (int v = 0; v < RR_TPB / 32; ++v) { a += s_w[v][threadIdx.x]; s_w[v][threadIdx.x] = 0; }
+      s_n[threadIdx.x] += a;
+    }
+    __syncthreads();
+  }
+  // level table: destination of (l, k) = P(l) + #{k' < k : N_k' > l}
+  int nmax = 0;
+  for (int k = 0; k < 32; ++k) nmax = max(nmax, s_n[k]);
+  const bool table = nmax <= RR_LEVELS;
+  if (table) {
+    for (int l = threadIdx.x; l < nmax; l += blockDim.x) {
+      int P = 0;
+      unsigned M = 0;
+      for (int k = 0; k < 32; ++k) {
+        const int n = s_n[k];
+        P += min(n, l);
+        M |= (n > l ? 1u : 0u) << k;
       }
-      bits[i][wd] = mk;
+      s_P[l] = P; s_M[l] = M;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
-      int acc = 0;
-      for (int wd = 0; wd < nw; ++wd) { wpre[i][wd] = acc; acc += __popc(bits[i][wd]); }
-      wpre[i][nw] = acc;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int c = s_carry;
-      for (int i = 0; i < nr; ++i) { base_r[i] = c; c += wpre[i][nw]; }
-      base_r[nr] = c;          // end of this pass's destinations
-      s_carry = c;
-    }
-    __syncthreads();
-    // destinations of this pass, in order: d -> rank i (binary search over
-    // the blocks), k-th cell of that rank in bank order (word prefix, then
-    // bit select), source through perm (cell-major slot)
-    const int dbeg = base_r[0], dend = base_r[nr];
-    for (int o = dbeg + threadIdx.x; o < dend; o += blockDim.x) {
-      int lo = 0, hi = nr - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (base_r[mid] <= o) lo = mid; else hi = mid - 1;
+  }
+  __syncthreads();
+  for (int sl = b0 + threadIdx.x; sl < b1; sl += blockDim.x) {
+    const int p = perm[sl];
+    const int lev = lev_at[sl], k = class_of(p);
+    int P = 0;
+    unsigned M = 0;
+    if (table) {
+      P = s_P[lev]; M = s_M[lev];
+    } else {
+      for (int k2 = 0; k2 < 32; ++k2) {
+        const int n = s_n[k2];
+        P += min(n, lev);
+        M |= (n > lev ? 1u : 0u) << k2;
       }
-      const int i = lo;
-      int k = o - base_r[i];
-      int wd = 0;
-      while (wd + 1 < nw && wpre[i][wd + 1] <= k) ++wd;
-      const int q = wd * 32 + select_bit(bits[i][wd], k - wpre[i][wd]);
-      const int lc = cell_at[q];
-      const int p = perm[b0 + pre[lc] + r0 + i];
-      const int d = b0 + o;
-      cell_dst[d] = __ldg(cell_src + p);
-      ox2[d] = __ldg(ox + p); oy2[d] = __ldg(oy + p); oz2[d] = __ldg(oz + p);
-      ux2[d] = __ldg(ux + p); uy2[d] = __ldg(uy + p); uz2[d] = __ldg(uz + p);
-      w2[d] = __ldg(w + p);
-      if (pid_src) pid_dst[d] = __ldg(pid_src + p);
     }
-    __syncthreads();
+    src_at[b0 + P + __popc(M & ((1u << k) - 1u))] = (uint32_t)p;
+  }
+  __syncthreads();
+  // gather in destination order (coalesced writes)
+  for (int d = b0 + threadIdx.x; d < b1; d += blockDim.x) {
+    const int p = (int)src_at[d];
+    src_at[d] = __ldg(cell + p);
+    ox2[d] = __ldg(ox + p); oy2[d] = __ldg(oy + p); oz2[d] = __ldg(oz + p);
+    ux2[d] = __ldg(ux + p); uy2[d] = __ldg(uy + p); uz2[d] = __ldg(uz + p);
+    w2[d] = __ldg(w + p);
+    if (pid_src) pid_dst[d] = __ldg(pid_src + p);
   }
 }
 
@@ -717,8 +683,9 @@ template <int ORDER>
 constexpr int reach_total() { return Reach<ORDER>::L + Reach<ORDER>::H; }
 
 int64_t smem_bytes(int order, int prec, int acc, int tx, int ty, int tz, int drift) {
-  int lh = order == 1 ? 1 : 3;
-  i64 V = (i64)(tx + 2 * drift + lh) * (ty + 2 * drift + lh) * (tz + 2 * drift + lh);
+  (void)ty; (void)tz;                 // cubic tiles
+  const int lh = order == 1 ? 1 : 3, W = tx + 2 * drift + lh;
+  const i64 V = (i64)pxrt::win_sz(tx, W) * W;
   i64 r = prec ? 8 : 4;
   i64 a = acc == 3 ? 8 : 4, nw = acc == 2 ? 2 : 1;
   return V * (6 * r + 3 * a * nw);

@@ -28,6 +28,21 @@ template <int ORDER> struct Reach {
   static constexpr int H = ORDER == 1 ? 1 : 2;
 };
 
+// Row and plane pitch (elements) of a tile's shared-memory window of edge W
+// for cubic tiles of edge T.  Padded so that the T^3 cells of the tile fall
+// into the 32 bank classes (address mod 32) exactly T^3/32 times each: the
+// sort lays out each warp's particles in distinct classes, and equal class
+// sizes let it do so for all but the tail of a tile.  Entries: smallest
+// window with that property, SY >= W, SZ >= SY * W.
+__host__ __device__ constexpr int win_sy(int T, int W) {
+  return T == 4 ? (W == 5 ? 6 : W == 7 ? 8 : W == 9 ? 10 : W) : W;
+}
+__host__ __device__ constexpr int win_sz(int T, int W) {
+  return T == 8 ? (W == 9 ? 84 : W == 11 ? 124 : W == 13 ? 172 : W == 15 ? 228 : W * W)
+       : T == 4 ? (W == 5 ? 40 : W == 7 ? 58 : W == 9 ? 104 : W * W)
+       : W * W;
+}
+
 // ---------------------------------------------------------------------------
 // Shapes from (cell, offset): x = c + o with o in [0,1).  r0 is the first
 // support node relative to c.  Same formulas as NodeShape/StagShape, with
@@ -234,9 +249,6 @@ __device__ __forceinline__ void cell_step(R& o, int& c, R du) {
   c += s;
 }
 
-template <typename R> __device__ __forceinline__ R rsqrt_(R x);
-template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return 1.0f / sqrtf(x); }
-template <> __device__ __forceinline__ double rsqrt_<double>(double x) { return 1.0 / sqrt(x); }
 
 // Shared-memory current accumulators (MODE):
 //  0  FP32 atomics;
@@ -483,7 +495,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     k_tile_step(const Job* __restrict__ jobs, const int2* __restrict__ work, int nwork,
                 const int* __restrict__ nwork_dev, int* ctr) {
   constexpr int L = Reach<ORDER>::L, H = Reach<ORDER>::H;
-  constexpr int W = T + 2 * D + L + H, SY = W, SZ = W * W, V = W * W * W;
+  constexpr int W = T + 2 * D + L + H, SY = win_sy(T, W), SZ = win_sz(T, W), V = SZ * W;
   typedef typename Acc<MODE>::T A;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* Fs = reinterpret_cast<R*>(smem_raw);
@@ -519,25 +531,25 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     const int tex = min(T, nx - c0x), tey = min(T, ny - c0y), tez = min(T, nz - c0z);
     const int wox = c0x - D - L, woy = c0y - D - L, woz = c0z - D - L;
     const int pbeg = sj.tile_off[tile], pend = sj.tile_off[tile + 1];
-    // ---- stage the E/B window; track |E|, |B| maxima -----------------------
+    // ---- stage the E/B window: asynchronous copies (cp.async), in flight
+    // while the accumulator is cleared and the tile's bounds are gathered ----
     const int pitch = sj.pitch_x, NYg = sj.pitch_y;
-    float emax = 0.f, bmax = 0.f;
     {
       const i64 base0 = (i64)(wox + G) + (i64)pitch * ((woy + G) + (i64)NYg * (woz + G));
 #pragma unroll 1
       for (int comp = 0; comp < 6; ++comp) {
         const R* src = (const R*)(comp == 0 ? sj.ex : comp == 1 ? sj.ey : comp == 2 ? sj.ez
                                  : comp == 3 ? sj.bx : comp == 4 ? sj.by : sj.bz) + base0;
-        R* dst = Fs + comp * V;
-        float m = 0.f;
-        for (int r = threadIdx.x; r < V; r += blockDim.x) {
-          const int a = r % W, b = (r / W) % W, c = r / SZ;
-          const R v = __ldg(src + a + (i64)pitch * (b + (i64)NYg * c));
-          dst[r] = v;
-          m = fmaxf(m, fabsf((float)v));
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(Fs + comp * V);
+        for (int r = threadIdx.x; r < W * W * W; r += blockDim.x) {
+          const int a = r % W, b = (r / W) % W, c = r / (W * W);
+          const R* g = src + a + (i64)pitch * (b + (i64)NYg * c);
+          const uint32_t d = dst + (uint32_t)((a + b * SY + c * SZ) * sizeof(R));
+          asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(g),
+                       "n"((int)sizeof(R)));
         }
-        if (comp < 3) emax = fmaxf(emax, m); else bmax = fmaxf(bmax, m);
       }
+      asm volatile("cp.async.commit_group;\n" ::);
     }
     for (int e = threadIdx.x; e < 3 * V * Acc<MODE>::NW; e += blockDim.x) Js[e] = (A)0;
     // ---- fixed-point scale of the current window (FP32 engine) -------------
@@ -574,6 +586,20 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
         cmax = fmaxf(cmax, (float)hist[r]);
         hist[r] = 0;
       }
+    }
+    // ---- window staged: |E|, |B| maxima ---------------------------------------
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    float emax = 0.f, bmax = 0.f;
+#pragma unroll 1
+    for (int comp = 0; comp < 6; ++comp) {
+      const R* f = Fs + comp * V;
+      float m = 0.f;
+      for (int r = threadIdx.x; r < W * W * W; r += blockDim.x) {
+        const int a = r % W, b = (r / W) % W, c = r / (W * W);
+        m = fmaxf(m, fabsf((float)f[a + b * SY + c * SZ]));
+      }
+      if (comp < 3) emax = fmaxf(emax, m); else bmax = fmaxf(bmax, m);
     }
     emax = warp_max(emax); bmax = warp_max(bmax); umax2 = warp_max(umax2); wmax = warp_max(wmax);
     cmax = warp_max(cmax);
@@ -660,7 +686,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       // ---- push ------------------------------------------------------------
       R gi;
       if (vay) {
-        gi = rsqrt_<R>((R)1 + (ux * ux + uy * uy + uz * uz) * clghtisq);
+        gi = inv_sqrt<R>((R)1 + (ux * ux + uy * uy + uz * uz) * clghtisq);
         vay_push(ux, uy, uz, gi, eb[0], eb[1], eb[2], eb[3], eb[4], eb[5], cst_v, invc, clghtisq);
       } else {
         boris_push(ux, uy, uz, gi, eb[0], eb[1], eb[2], eb[3], eb[4], eb[5], cst_b, clghtisq);
@@ -731,7 +757,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       // summed over the tile in FP64
       {
         const R u2 = (ux * ux + uy * uy + uz * uz) * clghtisq;
-        ke += (double)(u2 / ((R)1 + sqrt(u2 + (R)1)) * wgt);
+        ke += (double)(quot<R>(u2, (R)1 + sqrt(u2 + (R)1)) * wgt);
       }
     }
     __syncthreads();
@@ -768,10 +794,10 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
         double* dst = comp == 0 ? sj.jx : comp == 1 ? sj.jy : sj.jz;
         const double inv = 1.0 / (comp == 0 ? scale[0] : comp == 1 ? scale[1] : scale[2]);
         const A* src = Js + comp * V;
-        for (int r = threadIdx.x; r < V; r += blockDim.x) {
-          const double v = Acc<MODE>::get(src, r, 3 * V);
+        for (int r = threadIdx.x; r < W * W * W; r += blockDim.x) {
+          const int a = r % W, b = (r / W) % W, c = r / (W * W);
+          const double v = Acc<MODE>::get(src, a + b * SY + c * SZ, 3 * V);
           if (v == 0.0) continue;
-          const int a = r % W, b = (r / W) % W, c = r / SZ;
           const int gi = GlobAcc::wrap(wox + a, nx), gj = GlobAcc::wrap(woy + b, ny),
                     gk = GlobAcc::wrap(woz + c, nz);
           atomicAdd(dst + gi + (i64)nx * (gj + (i64)ny * gk), v * inv);
