@@ -279,17 +279,18 @@ int pxrb_tiled_push_e(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t pre
 
 /* Counting sort of one job's particles by cell tile: the B200 form of
  * pxr_particle_sorting (src/housekeeping/sorting.F90:67-361) with the tile of
- * the particle's cell as key.  Inside a tile the particles are laid out
- * round-robin over the tile's cells (every cell's first particle, then every
- * cell's second, ...), the cells ranked so that 32 consecutive ones fall in
- * distinct shared-memory banks of the tile window: a warp of the particle
- * kernel then touches 32 different cells without bank conflicts.  Rebuilds
+ * the particle's cell as key.  Inside a tile the particles are laid out in
+ * bank order: numbered within their bank class (the shared-memory bank of
+ * their cell in the tile window, whose pitch gives every class the same
+ * number of cells), then ordered by (number, class), so 32 consecutive
+ * particles fall in distinct banks: a warp of the particle kernel then
+ * gathers and deposits without bank conflicts until particles change cells.  Rebuilds
  * tile_off; the particle arrays keep their addresses (the *_b buffers, and
  * cell_cnt / rank_b / perm, are scratch).  job_host: host copy (sizes and pointers);
  * job_dev: the device copy the kernels read. */
 int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, void* stream);
 
-/* The same sort for a batch of jobs in five launches (an ensemble, the
+/* The same sort for a batch of jobs in seven launches (an ensemble, the
  * reference's per-species pxr_particle_sorting over many simulations).
  * jobs_dev: DEVICE array of njobs descriptors, all of precision `prec`, each
  * with cubic tiles of edge 4 or 8 and cell_cnt / rank_b / perm set; max_tiles: at
