@@ -7,8 +7,9 @@ component, order-3 shapes, Boris pusher, 8^3 cell tiles, re-sort every 20
 steps, 2nd-order Yee at 0.95 CFL, normalized units (c = mu0 = eps0 = 1,
 dx = 1), FP32 mixed precision (FP64 J flush and energy sums).  Synthetic
 seeded input stands in for the reference's decks.  A step is one full PIC
-step: fused gather/push/deposit kernel, B/E/B Yee pushes, and the periodic
-counting sort every 20 steps.
+step: fused gather/push/deposit kernel, B/E/B Yee pushes, the periodic
+counting sort every 20 steps, and between sorts a bank-order re-layout of
+each tile every 4 steps.
 
 Arms:
   (default)          this framework; also reports the plain FP64 GPU path,
@@ -41,11 +42,13 @@ WORKLOADS = {
     "large": dict(n=(256, 256, 256), ppc=8, order=3, tile=(8, 8, 8), sort_interval=20,
                   sigma=0.01, pusher=0,
                   desc="256^3 cells, 8 ppc (134,217,728 electrons), order 3, tiles 8^3, "
-                       "re-sort every 20 steps, Boris, u_th 0.01, periodic"),
+                       "re-sort every 20 steps (bank re-layout every 4 between), Boris, "
+                       "u_th 0.01, periodic"),
     "medium": dict(n=(128, 128, 64), ppc=8, order=3, tile=(8, 8, 8), sort_interval=20,
                    sigma=0.01, pusher=0,
                    desc="128x128x64 cells, 8 ppc (8,388,608 electrons), order 3, tiles 8^3, "
-                        "re-sort every 20 steps, Boris, u_th 0.01, periodic (profiling size)"),
+                        "re-sort every 20 steps (bank re-layout every 4 between), Boris, "
+                        "u_th 0.01, periodic (profiling size)"),
     "uneven": dict(n=(512, 128, 128), ppc=16, order=2, tile=(8, 8, 8), sort_interval=20,
                    sigma=0.005, u_drift=0.2, pusher=0, init="two_stream", autotune=True,
                    tune_sigma=0.2,
@@ -308,7 +311,8 @@ def run_ours(args):
     wl = WORKLOADS[args.workload]
     prec = 0 if args.precision == "fp32" else 1
     cfg = TiledConfig(tile=wl["tile"], sort_interval=wl["sort_interval"], drift=1,
-                      threads=args.threads, ctas_per_sm=args.ctas_per_sm, acc=args.acc)
+                      threads=args.threads, ctas_per_sm=args.ctas_per_sm, acc=args.acc,
+                      relayout_interval=args.relayout)
     tuned = None
     if wl.get("autotune"):
         from picsar_b200 import autotune
@@ -407,7 +411,8 @@ def run_ours(args):
                              f"{N * 32 / 1e9:.1f} GB per GPU), no flush",
                        "tuning": {"tile": list(wl["tile"]), "drift": cfg.drift,
                                   "threads": cfg.threads, "ctas_per_sm": cfg.ctas_per_sm,
-                                  "sort_interval": cfg.sort_interval, "acc": cfg.acc,
+                                  "sort_interval": cfg.sort_interval,
+                                  "relayout_interval": cfg.relayout_interval, "acc": cfg.acc,
                                   "autotuned": tuned},
                        "tile_occupancy": occupancy},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -458,7 +463,7 @@ def run_accuracy(wl, args, pusher, cfg):
     from picsar_b200.init import thermal_plasma
     from picsar_b200.tiled import TiledConfig, TiledSim
     cfg = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval, drift=cfg.drift,
-                      threads=cfg.threads, acc=cfg.acc)
+                      threads=cfg.threads, acc=cfg.acc, relayout_interval=cfg.relayout_interval)
     st = _initial_state(wl, 4321)
     steps = args.accuracy_steps
     sims, one = {}, {}
@@ -467,7 +472,8 @@ def run_accuracy(wl, args, pusher, cfg):
     cfg64 = cfg
     if (cfg.tile[0], cfg.drift) not in SUPPORTED_SHAPES_FP64:
         cfg64 = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval,
-                            drift=min(cfg.drift, 1), threads=cfg.threads)
+                            drift=min(cfg.drift, 1), threads=cfg.threads,
+                            relayout_interval=cfg.relayout_interval)
     for prec in ("fp64", "fp32"):
         t = TiledSim(wl["n"], order=wl["order"], pusher=pusher, precision=prec,
                      config=cfg64 if prec == "fp64" else cfg, track_ids=True)
@@ -609,6 +615,7 @@ def _tuned_configs(specs, precision="fp32"):
     dt = time.perf_counter() - t0
     info = {str(o): {"tile": r.config.tile[0], "drift": r.config.drift,
                      "threads": r.config.threads, "sort_interval": r.config.sort_interval,
+                     "relayout_interval": r.config.relayout_interval,
                      "proxy_rate": r.rate, "ppc": r.ppc, "sigma": r.sigma, "cached": r.cached}
             for o, r in tuned.items()}
     return {o: r.config for o, r in tuned.items()}, info, dt
@@ -622,7 +629,8 @@ def _with_acc(configs, acc):
     for o, c in configs.items():
         a = acc if acc in SUPPORTED_ACC.get((c.tile[0], c.drift), (2,)) else 2
         out[o] = TiledConfig(tile=c.tile, drift=c.drift, threads=c.threads,
-                             ctas_per_sm=c.ctas_per_sm, sort_interval=c.sort_interval, acc=a)
+                             ctas_per_sm=c.ctas_per_sm, sort_interval=c.sort_interval, acc=a,
+                             relayout_interval=c.relayout_interval)
     return out
 
 
@@ -824,6 +832,8 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--ctas-per-sm", type=int, default=2)
+    ap.add_argument("--relayout", type=int, default=4,
+                    help="bank re-layout interval between sorts (0: none), fixed workloads")
     ap.add_argument("--acc", type=int, default=1,
                     help="FP32 current accumulator: 1 int32 fixed point (default: energy drift "
                          "and Gauss residual within 1e-3 of FP64's, one-step field error "

@@ -277,6 +277,20 @@ int pxrb_tiled_push_e(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t pre
                       const int64_t* cell_off_dev, int64_t total_cells, int32_t zero_j,
                       void* stream);
 
+/* Bank-order re-layout of every tile of njobs jobs, between sorts: each
+ * tile's particles are put back into the sort's (level, bank class) order
+ * for the cells they occupy now (particles keep their tile).  A step's cost
+ * grows as particles change cells after a sort; this restores it for about
+ * a third of a sort's memory traffic.  The particles are gathered into the
+ * *_b buffers, which then trade places with the particle arrays in the
+ * DEVICE descriptors: read the current pointers back from there before
+ * using the arrays on the host side.  jobs_dev: DEVICE descriptors of
+ * precision `prec` (cubic tiles of edge 4 or 8); max_tiles: at least every
+ * job's tile count; max_np: the largest particle count (sizes the grid).
+ * rank_b is scratch. */
+int pxrb_tiled_relayout(pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
+                        int32_t max_tiles, int64_t max_np, void* stream);
+
 /* Counting sort of one job's particles by cell tile: the B200 form of
  * pxr_particle_sorting (src/housekeeping/sorting.F90:67-361) with the tile of
  * the particle's cell as key.  Inside a tile the particles are laid out in

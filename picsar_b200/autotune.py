@@ -6,9 +6,10 @@ jobs, a proxy simulation large enough to occupy every SM (at least two tiles
 per resident CTA) is stepped under each candidate and timed with CUDA events
 on the launching stream.  Stage 1 times every compiled (tile edge, margin)
 pair at both thread counts over 20 steps with a sort every 20 steps; stage 2
-times the winner at each sort interval over 40 steps (the slow path for
-particles that drifted out of their tile window, and the sort itself, both
-count).  Results are cached per GPU model in a JSON file
+times the winner at each pair of sort interval and bank re-layout interval
+over 40 steps (the slow path for particles that drifted out of their tile
+window, the bank conflicts of particles that changed cell, and the sorts
+and re-layouts themselves all count).  Results are cached per GPU model in a JSON file
 (``$PICSAR_B200_CACHE`` or ``~/.cache/picsar_b200/autotune.json``).
 
 The reference has no autotuner: its tile counts, vector lengths and
@@ -30,6 +31,7 @@ from .tiled import SUPPORTED_SHAPES, TiledConfig, TiledSim
 
 THREADS = (128, 256)
 SORT_INTERVALS = (5, 10, 20, 40)
+RELAYOUT_INTERVALS = (0, 2, 4)
 
 
 @dataclass
@@ -40,7 +42,7 @@ class TuneResult:
     sigma: float
     config: TiledConfig
     rate: float                     # particle-steps/s of the winner on the proxy
-    table: list = field(default_factory=list)   # (tile, drift, threads, sort, rate)
+    table: list = field(default_factory=list)   # (tile, drift, threads, sort, relayout, rate)
     cached: bool = False
 
 
@@ -54,7 +56,7 @@ def _cache_path():
 def _key(order, precision, ppc, sigma, pusher):
     name = torch.cuda.get_device_name()
     sb = round(math.log10(max(sigma, 1e-6)) * 2) / 2
-    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}|p{pusher}"
+    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}|p{pusher}|v2"
 
 
 def proxy_grid(ppc, num_sms, tile=8, ctas_per_sm=2):
@@ -87,7 +89,8 @@ def _time(cfg, order, precision, st, n, steps, pusher):
 
 
 def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
-         shapes=None, threads=THREADS, sort_intervals=SORT_INTERVALS, seed=7):
+         shapes=None, threads=THREADS, sort_intervals=SORT_INTERVALS,
+         relayout_intervals=RELAYOUT_INTERVALS, seed=7):
     """Best TiledConfig for jobs of this class, timed on a proxy simulation."""
     path = _cache_path()
     key = _key(order, precision, ppc, sigma, pusher)
@@ -110,23 +113,28 @@ def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
     best = None
     for edge, drift in shapes:
         for th in threads:
-            cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, threads=th, sort_interval=20)
+            cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, threads=th, sort_interval=20,
+                              relayout_interval=0)
             try:
                 r = _time(cfg, order, precision, st, n, 20, pusher)
             except (ValueError, RuntimeError, PicsarB200Error) as e:   # not compiled here
-                table.append((edge, drift, th, 20, None, str(e)[:80]))
+                table.append((edge, drift, th, 20, 0, None, str(e)[:80]))
                 continue
-            table.append((edge, drift, th, 20, r))
+            table.append((edge, drift, th, 20, 0, r))
             if best is None or r > best[1]:
                 best = (cfg, r)
     cfg0 = best[0]
     best = None
     for K in sort_intervals:
-        cfg = TiledConfig(tile=cfg0.tile, drift=cfg0.drift, threads=cfg0.threads, sort_interval=K)
-        r = _time(cfg, order, precision, st, n, 40, pusher)
-        table.append((cfg0.tile[0], cfg0.drift, cfg0.threads, K, r))
-        if best is None or r > best[1]:
-            best = (cfg, r)
+        for R in relayout_intervals:
+            if R >= K:
+                continue
+            cfg = TiledConfig(tile=cfg0.tile, drift=cfg0.drift, threads=cfg0.threads,
+                              sort_interval=K, relayout_interval=R)
+            r = _time(cfg, order, precision, st, n, 40, pusher)
+            table.append((cfg0.tile[0], cfg0.drift, cfg0.threads, K, R, r))
+            if best is None or r > best[1]:
+                best = (cfg, r)
     res = TuneResult(order, precision, ppc, sigma, best[0], best[1], table)
     if use_cache:
         try:

@@ -346,40 +346,182 @@ __global__ void k_sort_copy(const Job* __restrict__ jp) {
     ((unsigned char*)dst)[n16 * 16 + threadIdx.x] = ((const unsigned char*)src)[n16 * 16 + threadIdx.x];
 }
 
-// Bank-class layout of one tile (one CTA per tile).  The class of a particle
-// is the shared-memory window address of its stencil origin mod 32, i.e. of
-// its cell in the particle kernel's padded window pitch (at order 2 the
-// stencils start at the nearest node, so the cell is shifted by one along
-// each axis where the in-cell offset is >= 1/2).  The tile's particles,
-// taken cell-major, are numbered within their class (level) and laid out by
-// (level, class).  Every 32 consecutive particles then sit in distinct
-// classes, hence distinct banks for every gather load and deposit atomic of
-// a warp, until the smallest class runs out; only the tail beyond it repeats
-// classes, and cell-major numbering keeps those repeats mostly within one
-// cell (one address, a broadcast for the loads).
-constexpr int RR_TPB = 256;
+// Bank-class layout inside each tile.  The class of a particle is the
+// shared-memory window address of its stencil origin mod 32, i.e. of its cell
+// in the particle kernel's padded window pitch (at order 2 the stencils start
+// at the nearest node, so the cell is shifted by one along each axis where
+// the in-cell offset is >= 1/2).  The tile's particles, taken cell-major, are
+// numbered within their class (level) and laid out by (level, class): every
+// 32 consecutive particles then sit in distinct classes, hence distinct banks
+// for every gather load and deposit atomic of a warp, until the smallest
+// class runs out; only the tail beyond it repeats classes, and cell-major
+// numbering keeps those repeats mostly within one cell (one address, a
+// broadcast for the loads).  k_tile_map (below) computes the destinations,
+// k_relayout_gather moves the particles.
 constexpr int RR_MAXC = 512;        // cells per tile (tile edge <= 8)
-constexpr int RR_LEVELS = 2048;     // level table (larger classes: direct sums)
 
-template <typename R>
-__global__ void __launch_bounds__(RR_TPB) k_sort_rr(const Job* __restrict__ jp) {
+// Bank-order re-layout of every tile, between sorts (the tiles keep their
+// particle ranges).  Particles that changed cell since the last layout put
+// two lanes of a warp into one bank class, and the warp's window loads and
+// atomics then replay: with thermal motion the step's cost grows by about a
+// third within 20 steps.  This restores the sort's (level, class) order from
+// the particles' current cells: k_tile_map numbers the classes in the tile's
+// current order and finds every particle's destination; the gather then
+// moves the particles into the *_b buffers in destination order, and those
+// trade places with the particle arrays in the descriptors.
+
+// One warp per tile: classes numbered in input order with per-class counters
+// in shared memory (no block barriers), then the destination of every
+// particle from the level table, stored as the source of that destination.
+// CELL_MAJOR: the input order is the sort's cell-major permutation (perm);
+// otherwise the tile's current order.  Scratch: rank_b (level and class per
+// input slot); output: cell_b (source particle per destination).
+constexpr int TM_WARPS = 4;         // tiles per CTA
+constexpr int TM_LEVELS = 256;      // level table entries per tile
+constexpr int TM_SEG = 4096;        // classes staged per tile segment
+
+template <typename R, bool CELL_MAJOR>
+__global__ void __launch_bounds__(TM_WARPS * 32) k_tile_map(const Job* __restrict__ jp) {
+  __shared__ int s_cnt[TM_WARPS][32];
+  __shared__ int s_P[TM_WARPS][TM_LEVELS];
+  __shared__ unsigned s_M[TM_WARPS][TM_LEVELS];
+  __shared__ unsigned char s_cls[TM_WARPS][TM_SEG];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const Job& J = jp[blockIdx.y];
-  const int t = blockIdx.x;
-  if (t >= J.ntx * J.nty * J.ntz) return;
+  const int t = blockIdx.x * TM_WARPS + wid;
+  const int ntl = J.ntx * J.nty * J.ntz;
+  if (t >= ntl) return;                       // whole warp
   const int b0 = J.tile_off[t], b1 = J.tile_off[t + 1];
   if (b0 == b1) return;
-  __shared__ int s_n[32];                     // class sizes (running)
-  __shared__ int s_w[RR_TPB / 32][32];        // per-warp class counts of a chunk
-  __shared__ int s_P[RR_LEVELS];              // sum_k min(N_k, l)
-  __shared__ unsigned s_M[RR_LEVELS];         // classes k with N_k > l
-  const int T = J.tx;
+  const int T = J.tx, D = J.drift, nx = J.nx, ny = J.ny, nz = J.nz;
   const int L = J.order == 1 ? 0 : 1, H = J.order == 1 ? 1 : 2;
-  const int W = T + 2 * J.drift + L + H;
+  const int W = T + 2 * D + L + H;
   const int SY = pxrt::win_sy(T, W), SZ = pxrt::win_sz(T, W);
+  const int ntx = J.ntx, nty = J.nty;
+  const int x0 = (t % ntx) * T, y0 = ((t / ntx) % nty) * T, z0 = (t / (ntx * nty)) * T;
+  const int tex = min(T, nx - x0), tey = min(T, ny - y0), tez = min(T, nz - z0);
   const bool half = J.order == 2;
-  const int x0 = (t % J.ntx) * T, y0 = ((t / J.ntx) % J.nty) * T, z0 = (t / (J.ntx * J.nty)) * T;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint32_t* __restrict__ cell = J.cell;
+  const R* __restrict__ ox = (const R*)J.ox;
+  const R* __restrict__ oy = (const R*)J.oy;
+  const R* __restrict__ oz = (const R*)J.oz;
   const int* __restrict__ perm = J.perm;
+  int* key_at = J.rank_b;
+  uint32_t* src_at = J.cell_b;
+  int* cnt = s_cnt[wid];
+  auto source = [&](int sl) { return CELL_MAJOR ? __ldg(perm + sl) : sl; };
+  // class of a particle from its current cell (window-relative, periodic)
+  auto class_of = [&](int p) {
+    const uint32_t c = __ldg(cell + p);
+    int x = (int)(c & 2047u) - x0, y = (int)((c >> 11) & 2047u) - y0, z = (int)(c >> 22) - z0;
+    if (x > tex - 1 + D) x -= nx; else if (x < -D) x += nx;
+    if (y > tey - 1 + D) y -= ny; else if (y < -D) y += ny;
+    if (z > tez - 1 + D) z -= nz; else if (z < -D) z += nz;
+    if (half) {
+      x += __ldg(ox + p) >= (R)0.5 ? 1 : 0;
+      y += __ldg(oy + p) >= (R)0.5 ? 1 : 0;
+      z += __ldg(oz + p) >= (R)0.5 ? 1 : 0;
+    }
+    return (x + SY * y + SZ * z) & 31;
+  };
+  const bool packed = b1 - b0 < (1 << 26);    // level and class in one int
+  cnt[lane] = 0;
+  // per segment: the classes first (independent loads, several in flight)
+  // into shared memory, then the numbering pass over them in order
+  constexpr int U = 4;
+  unsigned char* cls = s_cls[wid];
+  for (int seg = b0; seg < b1; seg += TM_SEG) {
+    const int sn = min(TM_SEG, b1 - seg);
+    for (int i0 = 0; i0 < sn; i0 += 32 * U) {
+      int kk[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + 32 * u + lane;
+        kk[u] = i < sn ? class_of(source(seg + i)) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + 32 * u + lane;
+        if (i < sn) cls[i] = (unsigned char)kk[u];
+      }
+    }
+    __syncwarp();
+    for (int base = 0; base < sn; base += 32) {
+      const int i = base + lane;
+      const bool valid = i < sn;
+      const int k = valid ? (int)cls[i] : 32 + lane;
+      const unsigned peers = __match_any_sync(0xffffffffu, k);
+      const int lev = valid ? cnt[k] + __popc(peers & ((1u << lane) - 1u)) : 0;
+      __syncwarp();
+      if (valid && lane == __ffs(peers) - 1) cnt[k] += __popc(peers);
+      __syncwarp();
+      if (valid) key_at[seg + i] = packed ? (lev << 5 | k) : lev;
+    }
+    __syncwarp();
+  }
+  int nmax = cnt[lane];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+  const bool table = nmax <= TM_LEVELS;
+  auto level_row = [&](int l, int& P, unsigned& M) {
+    P = 0; M = 0;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const int c = cnt[k];
+      P += min(c, l);
+      M |= (c > l ? 1u : 0u) << k;
+    }
+  };
+  if (table) {
+    for (int l = lane; l < nmax; l += 32) level_row(l, s_P[wid][l], s_M[wid][l]);
+    __syncwarp();
+  }
+  for (int s0 = b0; s0 < b1; s0 += 32 * U) {
+    int kv[U], pp[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int sl = s0 + 32 * u + lane;
+      kv[u] = sl < b1 ? key_at[sl] : 0;
+      pp[u] = sl < b1 ? source(sl) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int sl = s0 + 32 * u + lane;
+      if (sl >= b1) continue;
+      const int lev = packed ? kv[u] >> 5 : kv[u], k = packed ? kv[u] & 31 : class_of(pp[u]);
+      int P;
+      unsigned M;
+      if (table) { P = s_P[wid][lev]; M = s_M[wid][lev]; }
+      else level_row(lev, P, M);
+      src_at[b0 + P + __popc(M & ((1u << k) - 1u))] = (uint32_t)pp[u];
+    }
+  }
+}
+
+// Exchange every job's particle arrays with their *_b buffers (after a
+// gather into the *_b buffers, instead of copying back).
+__global__ void k_swap_particle_buffers(pxrb_tiled_job* jp, int njobs) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  Job& J = jp[j];
+  { uint32_t* t = J.cell; J.cell = J.cell_b; J.cell_b = t; }
+  { void* t = J.ox; J.ox = J.ox_b; J.ox_b = t; }
+  { void* t = J.oy; J.oy = J.oy_b; J.oy_b = t; }
+  { void* t = J.oz; J.oz = J.oz_b; J.oz_b = t; }
+  { void* t = J.ux; J.ux = J.ux_b; J.ux_b = t; }
+  { void* t = J.uy; J.uy = J.uy_b; J.uy_b = t; }
+  { void* t = J.uz; J.uz = J.uz_b; J.uz_b = t; }
+  { void* t = J.w; J.w = J.w_b; J.w_b = t; }
+  if (J.pid) { int32_t* t = J.pid; J.pid = J.pid_b; J.pid_b = t; }
+}
+
+// Gather in destination order into the *_b buffers (all particles of a job):
+// the source of destination d is read from cell_b[d] before the cell
+// replaces it.
+template <typename R>
+__global__ void k_relayout_gather(const Job* __restrict__ jp) {
+  const Job J = jp[blockIdx.y];
+  const i64 np = J.np;
   const uint32_t* __restrict__ cell = J.cell;
   const R* __restrict__ ox = (const R*)J.ox;
   const R* __restrict__ oy = (const R*)J.oy;
@@ -388,89 +530,24 @@ __global__ void __launch_bounds__(RR_TPB) k_sort_rr(const Job* __restrict__ jp) 
   const R* __restrict__ uy = (const R*)J.uy;
   const R* __restrict__ uz = (const R*)J.uz;
   const R* __restrict__ w = (const R*)J.w;
-  R *ox2 = (R*)J.ox_b, *oy2 = (R*)J.oy_b, *oz2 = (R*)J.oz_b;
-  R *ux2 = (R*)J.ux_b, *uy2 = (R*)J.uy_b, *uz2 = (R*)J.uz_b, *w2 = (R*)J.w_b;
-  const int* __restrict__ pid_src = J.pid;
-  int* __restrict__ pid_dst = J.pid_b;
-  int* lev_at = J.rank_b;                     // level per cell-major slot
-  uint32_t* src_at = J.cell_b;                // source per destination, then its cell
-  auto class_of = [&](int p) {
-    const uint32_t c = __ldg(cell + p);
-    int x = (int)(c & 2047u) - x0, y = (int)((c >> 11) & 2047u) - y0, z = (int)(c >> 22) - z0;
-    if (half) {
-      x += __ldg(ox + p) >= (R)0.5 ? 1 : 0;
-      y += __ldg(oy + p) >= (R)0.5 ? 1 : 0;
-      z += __ldg(oz + p) >= (R)0.5 ? 1 : 0;
-    }
-    return (x + SY * y + SZ * z) & 31;
-  };
-  if (threadIdx.x < 32) s_n[threadIdx.x] = 0;
-  for (int e = threadIdx.x; e < 32 * (RR_TPB / 32); e += blockDim.x) (&s_w[0][0])[e] = 0;
-  __syncthreads();
-  // levels: running per-class counts over cell-major chunks of RR_TPB
-  for (int base = b0; base < b1; base += RR_TPB) {
-    const int sl = base + threadIdx.x;
-    const bool valid = sl < b1;
-    const int k = valid ? class_of(perm[sl]) : 32 + lane;    // distinct dummies
-    const unsigned peers = __match_any_sync(0xffffffffu, k);
-    const int inw = __popc(peers & ((1u << lane) - 1u));
-    if (valid && lane == __ffs(peers) - 1) s_w[wid][k] = __popc(peers);
-    __syncthreads();
-    if (valid) {
-      int lev = s_n[k] + inw;
-      for (int v = 0; v < wid; ++v) lev += s_w[v][k];
-      lev_at[sl] = lev;
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      int a = 0;
-      for (int v = 0; v < RR_TPB / 32; ++v) { a += s_w[v][threadIdx.x]; s_w[v][threadIdx.x] = 0; }
-      s_n[threadIdx.x] += a;
-    }
-    __syncthreads();
-  }
-  // level table: destination of (l, k) = P(l) + #{k' < k : N_k' > l}
-  int nmax = 0;
-  for (int k = 0; k < 32; ++k) nmax = max(nmax, s_n[k]);
-  const bool table = nmax <= RR_LEVELS;
-  if (table) {
-    for (int l = threadIdx.x; l < nmax; l += blockDim.x) {
-      int P = 0;
-      unsigned M = 0;
-      for (int k = 0; k < 32; ++k) {
-        const int n = s_n[k];
-        P += min(n, l);
-        M |= (n > l ? 1u : 0u) << k;
-      }
-      s_P[l] = P; s_M[l] = M;
-    }
-  }
-  __syncthreads();
-  for (int sl = b0 + threadIdx.x; sl < b1; sl += blockDim.x) {
-    const int p = perm[sl];
-    const int lev = lev_at[sl], k = class_of(p);
-    int P = 0;
-    unsigned M = 0;
-    if (table) {
-      P = s_P[lev]; M = s_M[lev];
-    } else {
-      for (int k2 = 0; k2 < 32; ++k2) {
-        const int n = s_n[k2];
-        P += min(n, lev);
-        M |= (n > lev ? 1u : 0u) << k2;
-      }
-    }
-    src_at[b0 + P + __popc(M & ((1u << k) - 1u))] = (uint32_t)p;
-  }
-  __syncthreads();
-  // gather in destination order (coalesced writes)
-  for (int d = b0 + threadIdx.x; d < b1; d += blockDim.x) {
-    const int p = (int)src_at[d];
-    src_at[d] = __ldg(cell + p);
-    ox2[d] = __ldg(ox + p); oy2[d] = __ldg(oy + p); oz2[d] = __ldg(oz + p);
-    ux2[d] = __ldg(ux + p); uy2[d] = __ldg(uy + p); uz2[d] = __ldg(uz + p);
-    w2[d] = __ldg(w + p);
-    if (pid_src) pid_dst[d] = __ldg(pid_src + p);
+  const int* __restrict__ pid = J.pid;
+  uint32_t* cb = J.cell_b;             // source per destination, then its cell
+  R* __restrict__ oxb = (R*)J.ox_b;
+  R* __restrict__ oyb = (R*)J.oy_b;
+  R* __restrict__ ozb = (R*)J.oz_b;
+  R* __restrict__ uxb = (R*)J.ux_b;
+  R* __restrict__ uyb = (R*)J.uy_b;
+  R* __restrict__ uzb = (R*)J.uz_b;
+  R* __restrict__ wb = (R*)J.w_b;
+  int* __restrict__ pidb = J.pid_b;
+  for (i64 d = blockIdx.x * (i64)blockDim.x + threadIdx.x; d < np;
+       d += (i64)gridDim.x * blockDim.x) {
+    const int p = (int)cb[d];
+    cb[d] = __ldg(cell + p);
+    oxb[d] = __ldg(ox + p); oyb[d] = __ldg(oy + p); ozb[d] = __ldg(oz + p);
+    uxb[d] = __ldg(ux + p); uyb[d] = __ldg(uy + p); uzb[d] = __ldg(uz + p);
+    wb[d] = __ldg(w + p);
+    if (pid) pidb[d] = __ldg(pid + p);
   }
 }
 
@@ -782,10 +859,12 @@ int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, voi
     if (!J.perm) return PXRB_EINVAL;
     k_sort_perm<<<nb, 256, 0, s>>>(job_dev);
     if (J.prec == 0) {
-      k_sort_rr<float><<<ntiles, RR_TPB, 0, s>>>(job_dev);
+      k_tile_map<float, true><<<(ntiles + TM_WARPS - 1) / TM_WARPS, TM_WARPS * 32, 0, s>>>(job_dev);
+      k_relayout_gather<float><<<nb, 256, 0, s>>>(job_dev);
       k_sort_copy<float><<<dim3(nb, 1, 9), 256, 0, s>>>(job_dev);
     } else {
-      k_sort_rr<double><<<ntiles, RR_TPB, 0, s>>>(job_dev);
+      k_tile_map<double, true><<<(ntiles + TM_WARPS - 1) / TM_WARPS, TM_WARPS * 32, 0, s>>>(job_dev);
+      k_relayout_gather<double><<<nb, 256, 0, s>>>(job_dev);
       k_sort_copy<double><<<dim3(nb, 1, 9), 256, 0, s>>>(job_dev);
     }
   }
@@ -804,7 +883,7 @@ int pxrb_tiled_sort_batch(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t
   const int64_t want = (max_np + 255) / 256;
   const int cap = njobs >= 4096 ? 1 : 4096 / njobs;
   const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
-  const dim3 g_np(bx, njobs), g_one(1, njobs), g_tiles(max_tiles, njobs);
+  const dim3 g_np(bx, njobs), g_one(1, njobs);
   const dim3 g_cs((max_tiles + CS_TPB / 32 - 1) / (CS_TPB / 32), njobs);
   k_sort_zero<<<g_np, 256, 0, s>>>(jobs_dev);
   k_sort_count<<<g_np, 256, 0, s>>>(jobs_dev);
@@ -812,12 +891,37 @@ int pxrb_tiled_sort_batch(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t
   k_sort_scan<<<g_one, SCAN_TPB, 0, s>>>(jobs_dev);
   k_sort_perm<<<g_np, 256, 0, s>>>(jobs_dev);
   if (prec == 0) {
-    k_sort_rr<float><<<g_tiles, RR_TPB, 0, s>>>(jobs_dev);
+    k_tile_map<float, true><<<dim3((max_tiles + TM_WARPS - 1) / TM_WARPS, njobs), TM_WARPS * 32, 0, s>>>(jobs_dev);
+    k_relayout_gather<float><<<g_np, 256, 0, s>>>(jobs_dev);
     k_sort_copy<float><<<dim3(g_np.x, njobs, 9), 256, 0, s>>>(jobs_dev);
   } else {
-    k_sort_rr<double><<<g_tiles, RR_TPB, 0, s>>>(jobs_dev);
+    k_tile_map<double, true><<<dim3((max_tiles + TM_WARPS - 1) / TM_WARPS, njobs), TM_WARPS * 32, 0, s>>>(jobs_dev);
+    k_relayout_gather<double><<<g_np, 256, 0, s>>>(jobs_dev);
     k_sort_copy<double><<<dim3(g_np.x, njobs, 9), 256, 0, s>>>(jobs_dev);
   }
+  PXRB_CHECK_LAUNCH();
+  return PXRB_OK;
+}
+
+int pxrb_tiled_relayout(pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
+                        int32_t max_tiles, int64_t max_np, void* stream) {
+  if (!jobs_dev || njobs < 1 || njobs > 65535 || max_tiles < 1 || max_np < 0)
+    return PXRB_EINVAL;
+  if (prec < 0 || prec > 1) return PXRB_EUNSUPPORTED;
+  if (max_np == 0) return PXRB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t want = (max_np + 255) / 256;
+  const int cap = njobs >= 4096 ? 1 : 4096 / njobs;
+  const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
+  const dim3 g_tiles((max_tiles + TM_WARPS - 1) / TM_WARPS, njobs), g_np(bx, njobs);
+  if (prec == 0) {
+    k_tile_map<float, false><<<g_tiles, TM_WARPS * 32, 0, s>>>(jobs_dev);
+    k_relayout_gather<float><<<g_np, 256, 0, s>>>(jobs_dev);
+  } else {
+    k_tile_map<double, false><<<g_tiles, TM_WARPS * 32, 0, s>>>(jobs_dev);
+    k_relayout_gather<double><<<g_np, 256, 0, s>>>(jobs_dev);
+  }
+  k_swap_particle_buffers<<<(njobs + 127) / 128, 128, 0, s>>>(jobs_dev, njobs);
   PXRB_CHECK_LAUNCH();
   return PXRB_OK;
 }

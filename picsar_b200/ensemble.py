@@ -14,7 +14,7 @@ device array and steps every job in a fixed set of launches:
     (``pxrb_tiled_sort_batch``).
 
 The per-step launches are captured once in a CUDA graph and replayed; the
-sorts have graphs of their own.  Jobs of one order share one tile shape,
+sorts and re-layouts have graphs of their own.  Jobs of one order share one tile shape,
 thread count and accumulator (template parameters of the particle kernel),
 chosen per order by ``picsar_b200.autotune``.
 
@@ -35,7 +35,7 @@ from . import _lib
 from .init import thermal_plasma
 from .tiled import TiledConfig, TiledJob, TiledSim, _stream
 
-_lib.register({"pxrb_tiled_sort_batch": "p I I I i s"})
+_lib.register({"pxrb_tiled_sort_batch": "p I I I i s", "pxrb_tiled_relayout": "p I I I i s"})
 
 
 @dataclass
@@ -181,8 +181,13 @@ class Ensemble:
         sz = C.sizeof(TiledJob)
         host = bytearray(sz * nj)
         for k, (sp, sim) in enumerate(self.members):
+            sim._pull_job()          # re-layouts may have exchanged its particle buffers
             host[k * sz:(k + 1) * sz] = bytes(sim.job)
         self.jobs_dev = torch.frombuffer(host, dtype=torch.uint8).to(self.device)
+        # each member's device descriptor is its slot of the packed array, so
+        # the member sees what the batched launches change there
+        for k, (sp, sim) in enumerate(self.members):
+            sim.job_dev = self.jobs_dev[k * sz:(k + 1) * sz]
         self.groups = []
         k = 0
         while k < nj:
@@ -235,6 +240,11 @@ class Ensemble:
         _lib.call("pxrb_tiled_sort_batch", self.jobs_dev.data_ptr() + grp.first * sz,
                   grp.count, self.prec, grp.max_tiles, grp.max_np, _stream())
 
+    def _launch_relayout(self, grp):
+        sz = C.sizeof(TiledJob)
+        _lib.call("pxrb_tiled_relayout", self.jobs_dev.data_ptr() + grp.first * sz,
+                  grp.count, self.prec, grp.max_tiles, grp.max_np, _stream())
+
     def _capture(self, fn):
         # warm up once on a side stream (sets kernel attributes), then capture
         side = torch.cuda.Stream(device=self.device)
@@ -245,6 +255,18 @@ class Ensemble:
                 fn()
         torch.cuda.current_stream().wait_stream(side)
         return g
+
+    def _run(self, key, fn):
+        """Run fn eagerly the first time, from its captured graph after."""
+        if not self.use_graph:
+            fn()
+            return
+        g = self._sort_graphs.get(key)
+        if g is None:
+            fn()
+            self._sort_graphs[key] = self._capture(fn)
+        else:
+            g.replay()
 
     def step(self, nsteps=1):
         """nsteps PIC steps of every job."""
@@ -262,19 +284,13 @@ class Ensemble:
             self.launches += len(self.groups) + 3
             self.it += 1
             for grp in self.groups:
-                K = grp.cfg.sort_interval
+                K, R = grp.cfg.sort_interval, grp.cfg.relayout_interval
                 if K > 0 and self.it % K == 0:
-                    if self.use_graph:
-                        g = self._sort_graphs.get(grp.order)
-                        if g is None:
-                            self._launch_sort(grp)
-                            self._sort_graphs[grp.order] = self._capture(
-                                lambda grp=grp: self._launch_sort(grp))
-                        else:
-                            g.replay()
-                    else:
-                        self._launch_sort(grp)
+                    self._run(("sort", grp.order), lambda grp=grp: self._launch_sort(grp))
                     self.launches += 7
+                elif R > 0 and self.it % R == 0 and grp.max_np > 0:
+                    self._run(("relayout", grp.order), lambda grp=grp: self._launch_relayout(grp))
+                    self.launches += 3
 
     # ------------------------------------------------------------ results
     def sims(self):

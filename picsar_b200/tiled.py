@@ -50,6 +50,7 @@ _lib.register({
     "pxrb_tiled_push_b": "p I I p i d s",
     "pxrb_tiled_push_e": "p I I p i I s",
     "pxrb_tiled_sort": "p p s",
+    "pxrb_tiled_relayout": "p I I I i s",
     "pxrb_tiled_load_particles": "p p p p p p p p s",
     "pxrb_tiled_store_particles": "p p p p p p p p p s",
     "pxrb_tiled_field_import": "p I p i s",
@@ -90,6 +91,7 @@ class TiledConfig:
     threads: int = 256
     ctas_per_sm: int = 2
     sort_interval: int = 20
+    relayout_interval: int = 4  # bank-order re-layout of the tiles between sorts (0: none)
     acc: int = 2                # FP32 engine current accumulator (see picsar_b200.h)
 
 
@@ -271,6 +273,26 @@ class TiledSim:
         _lib.call("pxrb_tiled_sort", self._jp(), self.job_dev.data_ptr(), _stream())
         self.launches += 6 if self.np > 0 else 1
 
+    def arrays(self):
+        """The particle arrays the device descriptor currently points at
+        (re-layouts exchange them with their scratch copies):
+        {"cell", "ox", "oy", "oz", "ux", "uy", "uz", "w"} tensors."""
+        self._pull_job()
+        j = self.job
+        out = {"cell": self.cell if self.cell.data_ptr() == j.cell else self.cell_b}
+        for c in ("ox", "oy", "oz", "ux", "uy", "uz", "w"):
+            a, b = self.parts[c], self.parts_b[c]
+            out[c] = a if a.data_ptr() == getattr(j, c) else b
+        return out
+
+    def relayout(self):
+        """Restore the bank order inside every tile for the particles' current
+        cells (particles keep their tiles)."""
+        if self.np > 0:
+            _lib.call("pxrb_tiled_relayout", self.job_dev.data_ptr(), 1, self.prec, self.ntiles,
+                      self.np, _stream())
+            self.launches += 3      # the particle arrays now sit in the former *_b buffers
+
     def particle_step(self):
         ctas = min(self.ntiles, self.num_sms * self.cfg.ctas_per_sm)
         _lib.call("pxrb_tiled_particle_step", self.job_dev.data_ptr(), self.order, self.prec,
@@ -312,6 +334,8 @@ class TiledSim:
             self.it += 1
             if self.cfg.sort_interval > 0 and self.it % self.cfg.sort_interval == 0:
                 self.sort()
+            elif self.cfg.relayout_interval > 0 and self.it % self.cfg.relayout_interval == 0:
+                self.relayout()
 
     # ----------------------------------------------------------- diagnostics
     def diagnostics(self, gauss=True, to_host=True):

@@ -7,7 +7,9 @@ particles within their bank class (cell-major) and lays them out by
 (level, class).  These tests rebuild the class of every sorted particle on
 the host and check the exact class sequence and the cell-major order inside
 each class, for orders 1-3 (order 2 shifts the class cell to the nearest
-node), 4^3 and 8^3 tiles, and a tile whose class outgrows the level table.
+node), 4^3 and 8^3 tiles, and a tile whose class outgrows the level table;
+and the same class sequence after particles moved and pxrb_tiled_relayout
+put each tile back in bank order (a permutation inside the tile).
 """
 import numpy as np
 import pytest
@@ -32,12 +34,17 @@ def test_pitch_table_gives_equal_bank_classes():
         assert h.min() == h.max() == T ** 3 // 32
 
 
-def _check(sim):
+def _check(sim, after_sort=True):
+    """after_sort: particles inside their tile, cell-major inside each class;
+    otherwise (after a re-layout of moved particles) within the tile window,
+    any order inside a class."""
     T = sim.tile[0]
+    D = sim.cfg.drift
     sy, sz = PITCH[(T, _window(T, sim.cfg.drift, sim.order))]
-    cell = sim.cell.cpu().numpy().astype(np.int64)
+    arr = sim.arrays()
+    cell = arr["cell"].cpu().numpy().astype(np.int64)
     off = sim.tile_off.cpu().numpy()
-    o = [sim.parts[c].cpu().numpy() for c in ("ox", "oy", "oz")]
+    o = [arr[c].cpu().numpy() for c in ("ox", "oy", "oz")]
     ntx, nty, _ = sim.nt
     x, y, z = cell & 2047, (cell >> 11) & 2047, cell >> 22
     checked = 0
@@ -46,11 +53,15 @@ def _check(sim):
         if b0 == b1:
             continue
         sl = slice(b0, b1)
-        lx = x[sl] - (t % ntx) * T
-        ly = y[sl] - ((t // ntx) % nty) * T
-        lz = z[sl] - (t // (ntx * nty)) * T
-        assert lx.min() >= 0 and lx.max() < T and ly.min() >= 0 and ly.max() < T
-        assert lz.min() >= 0 and lz.max() < T, "particle outside its tile"
+        loc = []
+        for v, t0, nn in ((x[sl], (t % ntx) * T, sim.n[0]), (y[sl], ((t // ntx) % nty) * T, sim.n[1]),
+                          (z[sl], (t // (ntx * nty)) * T, sim.n[2])):
+            lv = v - t0
+            lv = np.where(lv > T - 1 + D, lv - nn, np.where(lv < -D, lv + nn, lv))
+            lo, hi = (0, T - 1) if after_sort else (-D, T - 1 + D)
+            assert lv.min() >= lo and lv.max() <= hi, "particle outside its tile window"
+            loc.append(lv)
+        lx, ly, lz = loc
         hx, hy, hz = lx.copy(), ly.copy(), lz.copy()
         if sim.order == 2:
             hx += o[0][sl] >= 0.5
@@ -60,9 +71,10 @@ def _check(sim):
         n = np.bincount(k, minlength=32)
         want = np.array([c for lev in range(n.max()) for c in range(32) if n[c] > lev])
         assert np.array_equal(k, want), f"tile {t}: class sequence"
-        lc = lx + T * ly + T * T * lz
-        for c in range(32):
-            assert np.all(np.diff(lc[k == c]) >= 0), f"tile {t} class {c}: not cell-major"
+        if after_sort:
+            lc = lx + T * ly + T * T * lz
+            for c in range(32):
+                assert np.all(np.diff(lc[k == c]) >= 0), f"tile {t} class {c}: not cell-major"
         checked += 1
     return checked
 
@@ -89,7 +101,16 @@ def _sim(n, order, tile, drift, ppc, seed, prec="fp32", crowd=0):
 def test_layout_by_level_and_bank_class(cuda, order, tile, drift, prec):
     s = _sim((24, 16, 32), order, tile, drift, 8, 10 + order, prec)
     assert _check(s) == s.ntiles
-    s.step(3)                    # positions move; the next sort restores the layout
+    host = lambda d: {c: v.cpu().numpy() for c, v in d.items()}
+    s.step(3)                    # positions move; the re-layout restores the bank order
+    mid = host(s.particles())
+    s.relayout()
+    torch.cuda.synchronize()
+    assert _check(s, after_sort=False) == s.ntiles
+    after = host(s.particles())  # the same particles, permuted inside their tiles
+    key = lambda d: np.lexsort([d[c] for c in ("uz", "uy", "ux", "z", "y", "x")])
+    for c in mid:
+        assert np.array_equal(mid[c][key(mid)], after[c][key(after)]), c
     s.sort()
     torch.cuda.synchronize()
     assert _check(s) == s.ntiles
@@ -101,3 +122,8 @@ def test_layout_of_a_crowded_tile(cuda):
     # level table, summed directly)
     s = _sim((16, 16, 16), 3, 8, 1, 20, 5, crowd=70000)
     assert _check(s) == s.ntiles
+    s.step(1)
+    s.relayout()                 # a class beyond the level table: summed directly
+    torch.cuda.synchronize()
+    assert _check(s, after_sort=False) == s.ntiles
+    assert s.error_flag() == 0
