@@ -449,8 +449,14 @@ __global__ void __launch_bounds__(TM_WARPS * 32) k_tile_map(const Job* __restric
     for (int base = 0; base < sn; base += 32) {
       const int i = base + lane;
       const bool valid = i < sn;
-      const int k = valid ? (int)cls[i] : 32 + lane;
-      const unsigned peers = __match_any_sync(0xffffffffu, k);
+      const int k = valid ? (int)cls[i] : 0;
+      // lanes of the same class: five ballots over the class bits
+      unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+      for (int b = 0; b < 5; ++b) {
+        const unsigned m = __ballot_sync(0xffffffffu, (k >> b) & 1);
+        peers &= ((k >> b) & 1) ? m : ~m;
+      }
       const int lev = valid ? cnt[k] + __popc(peers & ((1u << lane) - 1u)) : 0;
       __syncwarp();
       if (valid && lane == __ffs(peers) - 1) cnt[k] += __popc(peers);
