@@ -223,6 +223,12 @@ typedef struct pxrb_tiled_job {
   int32_t* cell_cnt;                        /* sort scratch: ntiles * tile^3 */
   int32_t* rank_b;                          /* sort scratch: np */
   int32_t* perm;                            /* sort scratch: np */
+  float* tile_stats;                        /* NULL, or 4 per tile: the bounds of the
+                                               fixed-point current scale for the
+                                               next step (max |u|^2, max |w|, max
+                                               particles per window cell, valid);
+                                               written by each particle step,
+                                               invalidated by the sort */
 } pxrb_tiled_job;
 
 /* Tile shapes: cubic tiles of edge tx = ty = tz = `tile` in {4, 8} with window

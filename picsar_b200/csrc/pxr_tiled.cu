@@ -222,6 +222,10 @@ __global__ void k_sort_zero(const Job* __restrict__ jp) {
     if (i <= ntiles) J.tile_cnt[i] = 0;
     else J.cell_cnt[i - ntiles - 1] = 0;
   }
+  if (J.tile_stats)        // tiles get new particles: the carried bounds are void
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < 4 * ntiles;
+         i += (i64)gridDim.x * blockDim.x)
+      J.tile_stats[i] = 0.f;
 }
 
 __global__ void k_sort_count(const Job* __restrict__ jp) {
@@ -771,7 +775,8 @@ int64_t smem_bytes(int order, int prec, int acc, int tx, int ty, int tz, int dri
   const i64 V = (i64)pxrt::win_sz(tx, W) * W;
   i64 r = prec ? 8 : 4;
   i64 a = acc == 3 ? 8 : 4, nw = acc == 2 ? 2 : 1;
-  return V * (6 * r + 3 * a * nw);
+  const i64 hb = tx + 2 * drift;      // next-step occupancy histogram (fixed point)
+  return V * (6 * r + 3 * a * nw) + ((acc == 1 || acc == 2) ? hb * hb * hb * 4 : 0);
 }
 
 inline int gs_blocks(i64 n, int tpb) {
@@ -853,6 +858,9 @@ int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, voi
     return PXRB_EINVAL;
   if (cudaMemsetAsync(J.cell_cnt, 0, sizeof(int32_t) * (size_t)ntiles * J.tx * J.tx * J.tx, s) !=
       cudaSuccess)
+    return PXRB_ELAUNCH;
+  if (J.tile_stats && cudaMemsetAsync(J.tile_stats, 0, sizeof(float) * 4 * (size_t)ntiles, s) !=
+                          cudaSuccess)
     return PXRB_ELAUNCH;
   if (J.tx != 4 && J.tx != 8) return PXRB_EUNSUPPORTED;
   const int nb = gs_blocks(J.np, 256);

@@ -500,6 +500,11 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* Fs = reinterpret_cast<R*>(smem_raw);
   A* Js = reinterpret_cast<A*>(smem_raw + (size_t)6 * V * sizeof(R));
+  constexpr bool FIXED = MODE == 1 || MODE == 2;
+  // occupancy of the window cells after this step, for the next step's scale
+  constexpr int HB = T + 2 * D;
+  int* nh = reinterpret_cast<int*>(Js + 3 * V * Acc<MODE>::NW);
+  __shared__ int s_have;
   __shared__ Job sj;
   __shared__ int s_item;
   __shared__ int s_qn;
@@ -552,6 +557,10 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       asm volatile("cp.async.commit_group;\n" ::);
     }
     for (int e = threadIdx.x; e < 3 * V * Acc<MODE>::NW; e += blockDim.x) Js[e] = (A)0;
+    if (FIXED)
+      for (int e = threadIdx.x; e < HB * HB * HB; e += blockDim.x) nh[e] = 0;
+    float* stats = FIXED && sj.tile_stats ? sj.tile_stats + 4 * (size_t)tile : nullptr;
+    if (threadIdx.x == 0) s_have = stats && stats[3] != 0.f;
     // ---- fixed-point scale of the current window (FP32 engine) -------------
     // Bound of one particle's contribution to one node of J_c:
     //   |q| w_max / (dt dV / d_c) * (max displacement along c in cells),
@@ -560,11 +569,16 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     // A node of the window receives deposits only from particles whose old
     // cell lies within L+H+3 cells of it along every axis, so the node sum
     // is bounded by (max particles per window cell) * (L+H+3)^3 contributions.
+    // The bounds are carried from the previous step of this tile (written at
+    // its end for the same particles in their new cells), or, after a sort,
+    // taken by a pre-pass over the tile's particles.
     float umax2 = 0.f, wmax = 0.f, cmax = 0.f;
-    constexpr bool FIXED = MODE == 1 || MODE == 2;
-    if (FIXED) {
+    __syncthreads();
+    const bool have = FIXED && s_have;
+    if (have) {
+      umax2 = stats[0]; wmax = stats[1]; cmax = stats[2];
+    } else if (FIXED) {
       int* hist = reinterpret_cast<int*>(Js) + 2 * V;   // zero; re-zeroed below
-      __syncthreads();
       const R* uxp = (const R*)sj.ux; const R* uyp = (const R*)sj.uy;
       const R* uzp = (const R*)sj.uz; const R* wp = (const R*)sj.w;
       for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
@@ -649,6 +663,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     uint32_t* q_pk = sj.cell_b;
     R *q_ox = (R*)sj.ox_b, *q_oy = (R*)sj.oy_b, *q_oz = (R*)sj.oz_b;
     double ke = 0.0;
+    float nu2 = 0.f, nwm = 0.f;          // the next step's bounds (fixed point)
     int nslow = 0, bad = 0;
     __syncthreads();
 
@@ -753,6 +768,19 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       cellp[ip] = pack_cell(nci, ncj, nck);
       oxp[ip] = nox; oyp[ip] = noy; ozp[ip] = noz;
       uxp[ip] = ux; uyp[ip] = uy; uzp[ip] = uz;
+      if (FIXED && stats) {
+        // what the next step's pre-pass would find for this particle
+        int hx = nci - c0x, hy = ncj - c0y, hz = nck - c0z;
+        if (hx > tex - 1 + D) hx -= nx; else if (hx < -D) hx += nx;
+        if (hy > tey - 1 + D) hy -= ny; else if (hy < -D) hy += ny;
+        if (hz > tez - 1 + D) hz -= nz; else if (hz < -D) hz += nz;
+        if (hx >= -D && hx <= tex - 1 + D && hy >= -D && hy <= tey - 1 + D && hz >= -D &&
+            hz <= tez - 1 + D)
+          atomicAdd(nh + (hx + D) + (hy + D) * HB + (hz + D) * (HB * HB), 1);
+        const float a = (float)ux, b = (float)uy, c = (float)uz;
+        nu2 = fmaxf(nu2, a * a + b * b + c * c);
+        nwm = fmaxf(nwm, fabsf((float)wgt));
+      }
       // kinetic energy (gamma - 1) w of the particle in the engine's precision,
       // summed over the tile in FP64
       {
@@ -812,11 +840,25 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       if (lane == 0) s_red[wid] = v;
       if (nslow) atomicAdd(&sj.counters[0], nslow);
       if (bad) atomicExch(&sj.counters[1], 1);
+      if (FIXED && stats) {
+        float c = 0.f;
+        for (int r = threadIdx.x; r < HB * HB * HB; r += blockDim.x) c = fmaxf(c, (float)nh[r]);
+        c = warp_max(c);
+        const float a = warp_max(nu2), b = warp_max(nwm);
+        if (lane == 0) { s_max[0][wid] = a; s_max[1][wid] = b; s_max[2][wid] = c; }
+      }
       __syncthreads();
       if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < nwarps; ++w) t += s_red[w];
         sj.ke_tile[tile] = t * sj.m * sj.clight * sj.clight;
+        if (FIXED && stats) {
+          float a = 0.f, b = 0.f, c = 0.f;
+          for (int w = 0; w < nwarps; ++w) {
+            a = fmaxf(a, s_max[0][w]); b = fmaxf(b, s_max[1][w]); c = fmaxf(c, s_max[2][w]);
+          }
+          stats[0] = a; stats[1] = b; stats[2] = c; stats[3] = 1.f;
+        }
       }
     }
     __syncthreads();

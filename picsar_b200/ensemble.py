@@ -96,7 +96,7 @@ def job_bytes(spec: JobSpec, precision="fp32", config: TiledConfig | None = None
     pitch = -(-(nt[0] * t + 2 * g) // al) * al
     fcells = pitch * (nt[1] * t + 2 * g) * (nt[2] * t + 2 * g)
     ntiles = nt[0] * nt[1] * nt[2]
-    grid = 6 * fcells * r + 4 * spec.cells * 8 + ntiles * (t ** 3 * 4 + 16)
+    grid = 6 * fcells * r + 4 * spec.cells * 8 + ntiles * (t ** 3 * 4 + 32)
     parts = spec.particles * (2 * (7 * r + 4) + 8)
     return int(grid + parts + (1 << 16))
 

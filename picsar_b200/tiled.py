@@ -41,7 +41,8 @@ class TiledJob(C.Structure):
         + [(n, _P) for n in ("ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz", "cell", "ox",
                              "oy", "oz", "ux", "uy", "uz", "w", "cell_b", "ox_b", "oy_b", "oz_b",
                              "ux_b", "uy_b", "uz_b", "w_b", "pid", "pid_b", "tile_off",
-                             "tile_cnt", "ke_tile", "counters", "cell_cnt", "rank_b", "perm")]
+                             "tile_cnt", "ke_tile", "counters", "cell_cnt", "rank_b", "perm",
+                             "tile_stats")]
     )
 
 
@@ -149,6 +150,7 @@ class TiledSim:
         self.tile_off = torch.zeros(self.ntiles + 1, dtype=torch.int32, device=dev)
         self.tile_cnt = torch.zeros(self.ntiles + 1, dtype=torch.int32, device=dev)
         self.ke_tile = torch.zeros(self.ntiles, dtype=torch.float64, device=dev)
+        self.tile_stats = torch.zeros(self.ntiles * 4, dtype=torch.float32, device=dev)
         self.cell_cnt = torch.zeros(self.ntiles * tile[0] * tile[1] * tile[2], dtype=torch.int32,
                                     device=dev)
         self.counters = torch.zeros(4, dtype=torch.int32, device=dev)
@@ -195,6 +197,7 @@ class TiledSim:
         j.tile_off, j.tile_cnt = self.tile_off.data_ptr(), self.tile_cnt.data_ptr()
         j.ke_tile, j.counters = self.ke_tile.data_ptr(), self.counters.data_ptr()
         j.cell_cnt = self.cell_cnt.data_ptr()
+        j.tile_stats = self.tile_stats.data_ptr()
         self._push_job()
 
     def _jp(self):
@@ -401,7 +404,7 @@ class TiledSim:
         """Device bytes held by this simulation."""
         tot = 0
         for t in self.E + self.B + self.J + [self.rho, self.tile_off, self.tile_cnt,
-                                             self.ke_tile]:
+                                             self.ke_tile, self.tile_stats]:
             tot += t.numel() * t.element_size()
         if self.np:
             tot += sum(t.numel() * t.element_size() for t in self.parts.values()) * 2
