@@ -51,7 +51,6 @@ WORKLOADS = {
                         "u_th 0.01, periodic (profiling size)"),
     "uneven": dict(n=(512, 128, 128), ppc=16, order=2, tile=(8, 8, 8), sort_interval=20,
                    sigma=0.005, u_drift=0.2, pusher=0, init="two_stream", autotune=True,
-                   tune_sigma=0.2,
                    desc="512x128x128 cells, density ramp 0->1 over x in [0,256) then flat, "
                         "16 ppc at n0 (~100.7 M electrons), two beams u_x=+-0.2 with u_th "
                         "0.005, order 2, Boris, periodic, autotuned tiles and sort interval"),
@@ -316,7 +315,8 @@ def run_ours(args):
     tuned = None
     if wl.get("autotune"):
         from picsar_b200 import autotune
-        r = autotune.tune(wl["order"], args.precision, ppc=wl["ppc"], sigma=wl["tune_sigma"],
+        r = autotune.tune(wl["order"], args.precision, ppc=wl["ppc"], sigma=wl["sigma"],
+                          u_drift=wl.get("u_drift", 0.0),
                           pusher=wl["pusher"])
         cfg = _with_acc({0: r.config}, args.acc)[0]
         tuned = {"proxy_rate": r.rate, "cached": r.cached}

@@ -5,7 +5,7 @@ For a (shape order, precision, particles per cell, thermal spread) class of
 jobs, a proxy simulation large enough to occupy every SM (at least two tiles
 per resident CTA) is stepped under each candidate and timed with CUDA events
 on the launching stream.  Stage 1 times every compiled (tile edge, margin)
-pair at both thread counts over 20 steps with a sort every 20 steps; stage 2
+pair at both thread counts over 20 steps with a sort every 5 steps; stage 2
 times the two best at each pair of sort interval and bank re-layout interval
 over 40 steps (the slow path for particles that drifted out of their tile
 window, the bank conflicts of particles that changed cell, and the sorts
@@ -53,10 +53,11 @@ def _cache_path():
     return os.path.join(os.path.expanduser("~"), ".cache", "picsar_b200", "autotune.json")
 
 
-def _key(order, precision, ppc, sigma, pusher):
+def _key(order, precision, ppc, sigma, pusher, u_drift=0.0):
     name = torch.cuda.get_device_name()
     sb = round(math.log10(max(sigma, 1e-6)) * 2) / 2
-    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}|p{pusher}|v3"
+    db = f"|d{round(u_drift, 2)}" if u_drift else ""
+    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}{db}|p{pusher}|v4"
 
 
 def proxy_grid(ppc, num_sms, tile=8, ctas_per_sm=2):
@@ -90,10 +91,12 @@ def _time(cfg, order, precision, st, n, steps, pusher):
 
 def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
          shapes=None, threads=THREADS, sort_intervals=SORT_INTERVALS,
-         relayout_intervals=RELAYOUT_INTERVALS, seed=7):
-    """Best TiledConfig for jobs of this class, timed on a proxy simulation."""
+         relayout_intervals=RELAYOUT_INTERVALS, seed=7, u_drift=0.0):
+    """Best TiledConfig for jobs of this class, timed on a proxy simulation
+    (thermal spread sigma; u_drift > 0: two counter-streaming beams u_x =
+    +-u_drift, as in a two-stream plasma)."""
     path = _cache_path()
-    key = _key(order, precision, ppc, sigma, pusher)
+    key = _key(order, precision, ppc, sigma, pusher, u_drift)
     if use_cache and os.path.exists(path):
         try:
             with open(path) as f:
@@ -107,20 +110,25 @@ def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
     props = torch.cuda.get_device_properties(torch.cuda.current_device())
     n = proxy_grid(ppc, props.multi_processor_count)
     st = thermal_plasma(n, ppc, sigma, seed=seed, device="cuda")
+    if u_drift:
+        st.ux[0::2] += u_drift
+        st.ux[1::2] -= u_drift
     if shapes is None:
         shapes = sorted(SUPPORTED_SHAPES)
     table = []
     ranked = []
     for edge, drift in shapes:
         for th in threads:
-            cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, threads=th, sort_interval=20,
+            # a short sort interval, so that shapes are ranked by the kernel
+            # rather than by the slow path of particles that left their window
+            cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, threads=th, sort_interval=5,
                               relayout_interval=0)
             try:
                 r = _time(cfg, order, precision, st, n, 20, pusher)
             except (ValueError, RuntimeError, PicsarB200Error) as e:   # not compiled here
-                table.append((edge, drift, th, 20, 0, None, str(e)[:80]))
+                table.append((edge, drift, th, 5, 0, None, str(e)[:80]))
                 continue
-            table.append((edge, drift, th, 20, 0, r))
+            table.append((edge, drift, th, 5, 0, r))
             ranked.append((r, cfg))
     # stage 2 for the two best (shape, threads) pairs of stage 1: a shape that
     # loses at the stage-1 sort interval can win at another
