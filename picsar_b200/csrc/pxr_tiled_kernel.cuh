@@ -513,6 +513,12 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 
   if (nwork_dev) nwork = min(nwork, *nwork_dev);
+  // the window's pitch padding is never staged: zero it once, so that whole
+  // components can be scanned without decoding window coordinates
+  for (int r = threadIdx.x; r < 6 * V; r += blockDim.x) {
+    const int q = r % V, c = q / SZ, b = (q - c * SZ) / SY, a = q - c * SZ - b * SY;
+    if (a >= W || b >= W) Fs[r] = (R)0;
+  }
   for (;;) {
     if (threadIdx.x == 0) {
       s_item = atomicAdd(ctr, 1);
@@ -605,15 +611,9 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     float emax = 0.f, bmax = 0.f;
-#pragma unroll 1
-    for (int comp = 0; comp < 6; ++comp) {
-      const R* f = Fs + comp * V;
-      float m = 0.f;
-      for (int r = threadIdx.x; r < W * W * W; r += blockDim.x) {
-        const int a = r % W, b = (r / W) % W, c = r / (W * W);
-        m = fmaxf(m, fabsf((float)f[a + b * SY + c * SZ]));
-      }
-      if (comp < 3) emax = fmaxf(emax, m); else bmax = fmaxf(bmax, m);
+    for (int r = threadIdx.x; r < 3 * V; r += blockDim.x) {
+      emax = fmaxf(emax, fabsf((float)Fs[r]));
+      bmax = fmaxf(bmax, fabsf((float)Fs[r + 3 * V]));
     }
     emax = warp_max(emax); bmax = warp_max(bmax); umax2 = warp_max(umax2); wmax = warp_max(wmax);
     cmax = warp_max(cmax);
@@ -822,10 +822,10 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
         double* dst = comp == 0 ? sj.jx : comp == 1 ? sj.jy : sj.jz;
         const double inv = 1.0 / (comp == 0 ? scale[0] : comp == 1 ? scale[1] : scale[2]);
         const A* src = Js + comp * V;
-        for (int r = threadIdx.x; r < W * W * W; r += blockDim.x) {
-          const int a = r % W, b = (r / W) % W, c = r / (W * W);
-          const double v = Acc<MODE>::get(src, a + b * SY + c * SZ, 3 * V);
-          if (v == 0.0) continue;
+        for (int r = threadIdx.x; r < V; r += blockDim.x) {
+          const double v = Acc<MODE>::get(src, r, 3 * V);
+          if (v == 0.0) continue;               // includes the pitch padding
+          const int c = r / SZ, b = (r - c * SZ) / SY, a = r - c * SZ - b * SY;
           const int gi = GlobAcc::wrap(wox + a, nx), gj = GlobAcc::wrap(woy + b, ny),
                     gk = GlobAcc::wrap(woz + c, nz);
           atomicAdd(dst + gi + (i64)nx * (gj + (i64)ny * gk), v * inv);
