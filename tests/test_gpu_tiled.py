@@ -175,3 +175,38 @@ def test_golden_fixtures_fp64(cuda):
             ref = fx[f"{tag}/{c}"]
             dxp = (got[c] - ref + L / 2) % L - L / 2
             assert np.linalg.norm(dxp) / np.linalg.norm(ref) <= 1e-12, (tag, c)
+
+
+@pytest.mark.parametrize("acc", [1, 2])
+def test_carried_tile_bounds_match_prepass(cuda, acc):
+    """The fixed-point bounds each tile carries to the next step equal what a
+    pre-pass over the tile's particles finds: a job descriptor without
+    tile_stats (pre-pass every step) gives the same state after 6 steps.
+    The scales can differ only by FMA contraction in max |u|^2, so the states
+    differ by the accumulator's quantisation: 1e-5 relative with one int32
+    word (mode 1), 1e-6 with two (mode 2)."""
+    tol = 1e-5 if acc == 1 else 1e-6
+    n = (24, 16, 32)
+    st = plasma(n, 4, 0.05, seed=31)
+    fields = random_fields(n, 3, seed=7, amp=0.02)
+    sims = []
+    for carried in (True, False):
+        t = TiledSim(n, order=3, precision="fp32",
+                     config=TiledConfig(tile=(8, 8, 8), acc=acc, relayout_interval=2),
+                     track_ids=True)
+        for name, a in zip(FIELDS, fields):
+            t.import_field(name, P.to_fortran(a), 3)
+        if not carried:
+            t.job.tile_stats = None
+            t._push_job()
+        t.load_particles(st["x"], st["y"], st["z"], st["ux"], st["uy"], st["uz"], st["w"])
+        t.step(6, keep_j=True)
+        sims.append(t)
+    torch.cuda.synchronize()
+    assert sims[0].tile_stats.view(-1, 4)[:, 3].min().item() == 1.0   # every tile carries
+    for name in FIELDS + ("jx", "jy", "jz"):
+        a, b = (s.export_field(name, 3).cpu().numpy() for s in sims)
+        assert rel_l2(a, b) <= tol, name
+    pa, pb = ({k: v.cpu().numpy() for k, v in s.particles().items()} for s in sims)
+    for c in ("ux", "uy", "uz"):
+        assert rel_l2(pa[c], pb[c]) <= tol, c
