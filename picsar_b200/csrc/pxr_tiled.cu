@@ -193,9 +193,9 @@ __global__ void __launch_bounds__(YEE_TPB)
 //   scan:     tile totals -> tile_off;
 //   perm:     perm[tile_off + prefix(cell) + rank] = p (cell-major order
 //             inside the tile; only a 4-byte index moves);
-//   rr:       per tile, walks its round-robin destinations in order, finds
-//             each one's (cell, rank) and source p through perm, and gathers
-//             the particle into the *_b buffers (coalesced writes);
+//   map:      per tile (one warp), the bank-order destination of every
+//             particle (k_tile_map, below), stored as its source in cell_b;
+//   gather:   in destination order into the *_b buffers (coalesced writes);
 //   copy:     *_b -> primary arrays (coalesced).
 // ---------------------------------------------------------------------------
 struct TileCell {
