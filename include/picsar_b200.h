@@ -304,10 +304,13 @@ int pxrb_tiled_relayout(pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
  * their cell in the tile window, whose pitch gives every class the same
  * number of cells), then ordered by (number, class), so 32 consecutive
  * particles fall in distinct banks: a warp of the particle kernel then
- * gathers and deposits without bank conflicts until particles change cells.  Rebuilds
- * tile_off; the particle arrays keep their addresses (the *_b buffers, and
- * cell_cnt / rank_b / perm, are scratch).  job_host: host copy (sizes and pointers);
- * job_dev: the device copy the kernels read. */
+ * gathers and deposits without bank conflicts until particles change cells.
+ * Rebuilds tile_off.  The sorted particles land in the *_b buffers, which then
+ * trade places with the particle arrays in the DEVICE descriptor (as in
+ * pxrb_tiled_relayout): read the particle pointers back from there before
+ * using the arrays on the host side.  cell_cnt / rank_b / perm are scratch.
+ * job_host: host copy (sizes and scratch pointers); job_dev: the device copy
+ * the kernels read and update. */
 int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, void* stream);
 
 /* The same sort for a batch of jobs in seven launches (an ensemble, the
@@ -316,8 +319,9 @@ int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, voi
  * with cubic tiles of edge 4 or 8 and cell_cnt / rank_b / perm set; max_tiles: at
  * least the tile count of every job; max_np: the largest particle count
  * (sizes the grid only).  The counters are cleared on the device, so the
- * call needs no host copy of the descriptors. */
-int pxrb_tiled_sort_batch(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
+ * call needs no host copy of the descriptors; the particle arrays trade
+ * places with the *_b buffers in the descriptors, as in the single sort. */
+int pxrb_tiled_sort_batch(pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
                           int32_t max_tiles, int64_t max_np, void* stream);
 
 /* Conversions between PICSAR's particle arrays (absolute FP64 positions,

@@ -195,8 +195,9 @@ __global__ void __launch_bounds__(YEE_TPB)
 //             inside the tile; only a 4-byte index moves);
 //   map:      per tile (one warp), the bank-order destination of every
 //             particle (k_tile_map, below), stored as its source in cell_b;
-//   gather:   in destination order into the *_b buffers (coalesced writes);
-//   copy:     *_b -> primary arrays (coalesced).
+//   gather:   in destination order into the *_b buffers (coalesced writes),
+//             which then trade places with the particle arrays in the
+//             device descriptors (k_swap_particle_buffers).
 // ---------------------------------------------------------------------------
 struct TileCell {
   int t, lc;
@@ -315,39 +316,6 @@ __global__ void k_sort_perm(const Job* __restrict__ jp) {
     const TileCell tc = tile_cell(J, cell[p]);
     perm[toff[tc.t] + cc[(i64)tc.t * T3 + tc.lc] + rank[p]] = (int)p;
   }
-}
-
-// One array per blockIdx.z (cell, 7 reals, pid): a plain coalesced copy.
-template <typename R>
-__global__ void k_sort_copy(const Job* __restrict__ jp) {
-  const Job J = jp[blockIdx.y];
-  const i64 np = J.np;
-  const int a = blockIdx.z;
-  const void* src;
-  void* dst;
-  int es = sizeof(R);
-  switch (a) {
-    case 0: src = J.cell_b; dst = J.cell; es = 4; break;
-    case 1: src = J.ox_b; dst = J.ox; break;
-    case 2: src = J.oy_b; dst = J.oy; break;
-    case 3: src = J.oz_b; dst = J.oz; break;
-    case 4: src = J.ux_b; dst = J.ux; break;
-    case 5: src = J.uy_b; dst = J.uy; break;
-    case 6: src = J.uz_b; dst = J.uz; break;
-    case 7: src = J.w_b; dst = J.w; break;
-    default: src = J.pid_b; dst = J.pid; es = 4; break;
-  }
-  if (!src || !dst) return;
-  // 16-byte chunks (torch allocations are 256-byte aligned), then the tail
-  const i64 bytes = np * es, n16 = bytes / 16;
-  const uint4* __restrict__ s4 = (const uint4*)src;
-  uint4* __restrict__ d4 = (uint4*)dst;
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n16;
-       i += (i64)gridDim.x * blockDim.x)
-    d4[i] = __ldg(s4 + i);
-  const i64 tail = bytes - n16 * 16;
-  if (blockIdx.x == 0 && threadIdx.x < tail)
-    ((unsigned char*)dst)[n16 * 16 + threadIdx.x] = ((const unsigned char*)src)[n16 * 16 + threadIdx.x];
 }
 
 // Bank-class layout inside each tile.  The class of a particle is the
@@ -875,18 +843,17 @@ int pxrb_tiled_sort(const pxrb_tiled_job* job_host, pxrb_tiled_job* job_dev, voi
     if (J.prec == 0) {
       k_tile_map<float, true><<<(ntiles + TM_WARPS - 1) / TM_WARPS, TM_WARPS * 32, 0, s>>>(job_dev);
       k_relayout_gather<float><<<nb, 256, 0, s>>>(job_dev);
-      k_sort_copy<float><<<dim3(nb, 1, 9), 256, 0, s>>>(job_dev);
     } else {
       k_tile_map<double, true><<<(ntiles + TM_WARPS - 1) / TM_WARPS, TM_WARPS * 32, 0, s>>>(job_dev);
       k_relayout_gather<double><<<nb, 256, 0, s>>>(job_dev);
-      k_sort_copy<double><<<dim3(nb, 1, 9), 256, 0, s>>>(job_dev);
     }
+    k_swap_particle_buffers<<<1, 32, 0, s>>>(job_dev, 1);
   }
   PXRB_CHECK_LAUNCH();
   return PXRB_OK;
 }
 
-int pxrb_tiled_sort_batch(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
+int pxrb_tiled_sort_batch(pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t prec,
                           int32_t max_tiles, int64_t max_np, void* stream) {
   if (!jobs_dev || njobs < 1 || njobs > 65535 || max_tiles < 1 || max_np < 0)
     return PXRB_EINVAL;
@@ -907,12 +874,11 @@ int pxrb_tiled_sort_batch(const pxrb_tiled_job* jobs_dev, int32_t njobs, int32_t
   if (prec == 0) {
     k_tile_map<float, true><<<dim3((max_tiles + TM_WARPS - 1) / TM_WARPS, njobs), TM_WARPS * 32, 0, s>>>(jobs_dev);
     k_relayout_gather<float><<<g_np, 256, 0, s>>>(jobs_dev);
-    k_sort_copy<float><<<dim3(g_np.x, njobs, 9), 256, 0, s>>>(jobs_dev);
   } else {
     k_tile_map<double, true><<<dim3((max_tiles + TM_WARPS - 1) / TM_WARPS, njobs), TM_WARPS * 32, 0, s>>>(jobs_dev);
     k_relayout_gather<double><<<g_np, 256, 0, s>>>(jobs_dev);
-    k_sort_copy<double><<<dim3(g_np.x, njobs, 9), 256, 0, s>>>(jobs_dev);
   }
+  k_swap_particle_buffers<<<(njobs + 127) / 128, 128, 0, s>>>(jobs_dev, njobs);
   PXRB_CHECK_LAUNCH();
   return PXRB_OK;
 }

@@ -274,18 +274,21 @@ class TiledSim:
         # sizes, tile_cnt and tile_off of the host descriptor never change;
         # the particle pointers it holds may be stale (the device swaps them)
         _lib.call("pxrb_tiled_sort", self._jp(), self.job_dev.data_ptr(), _stream())
-        self.launches += 6 if self.np > 0 else 1
+        self.launches += 7 if self.np > 0 else 1   # the particle arrays now sit in the former *_b buffers
 
     def arrays(self):
         """The particle arrays the device descriptor currently points at
-        (re-layouts exchange them with their scratch copies):
-        {"cell", "ox", "oy", "oz", "ux", "uy", "uz", "w"} tensors."""
+        (sorts and re-layouts exchange them with their scratch copies):
+        {"cell", "ox", "oy", "oz", "ux", "uy", "uz", "w"} tensors, and "pid"
+        when ids are tracked."""
         self._pull_job()
         j = self.job
         out = {"cell": self.cell if self.cell.data_ptr() == j.cell else self.cell_b}
         for c in ("ox", "oy", "oz", "ux", "uy", "uz", "w"):
             a, b = self.parts[c], self.parts_b[c]
             out[c] = a if a.data_ptr() == getattr(j, c) else b
+        if self.track_ids and j.pid:
+            out["pid"] = self.pid if self.pid.data_ptr() == j.pid else self.pid_b
         return out
 
     def relayout(self):

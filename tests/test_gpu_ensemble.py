@@ -97,12 +97,10 @@ def test_batched_sort_layout_matches_single_job_sort(cuda):
     ens.step(1)                          # one step, then the batched sort
     for spec, sim in ens.sims():
         off_b = sim.tile_off.cpu().numpy().copy()
-        pid_b = sim.pid.cpu().numpy().copy() if sim.job.pid == sim.pid.data_ptr() else \
-            sim.pid_b.cpu().numpy().copy()
+        pid_b = sim.arrays()["pid"].cpu().numpy().copy()
         sim.sort()                       # single-job path on the same state
         off_s = sim.tile_off.cpu().numpy()
-        pid_s = sim.pid.cpu().numpy() if sim.job.pid == sim.pid.data_ptr() else \
-            sim.pid_b.cpu().numpy()
+        pid_s = sim.arrays()["pid"].cpu().numpy()
         assert np.array_equal(off_b, off_s)
         for t in range(sim.ntiles):
             a, b = off_s[t], off_s[t + 1]
