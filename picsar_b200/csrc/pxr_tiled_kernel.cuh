@@ -562,7 +562,17 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       }
       asm volatile("cp.async.commit_group;\n" ::);
     }
-    for (int e = threadIdx.x; e < 3 * V * Acc<MODE>::NW; e += blockDim.x) Js[e] = (A)0;
+    {
+      // 16-byte stores where the accumulator's size and offset allow
+      constexpr size_t JB = (size_t)3 * V * Acc<MODE>::NW * sizeof(A);
+      constexpr bool VEC = JB % 16 == 0 && ((size_t)6 * V * sizeof(R)) % 16 == 0;
+      if (VEC) {
+        uint4* j4 = reinterpret_cast<uint4*>(Js);
+        for (int e = threadIdx.x; e < (int)(JB / 16); e += blockDim.x) j4[e] = make_uint4(0, 0, 0, 0);
+      } else {
+        for (int e = threadIdx.x; e < 3 * V * Acc<MODE>::NW; e += blockDim.x) Js[e] = (A)0;
+      }
+    }
     if (FIXED)
       for (int e = threadIdx.x; e < HB * HB * HB; e += blockDim.x) nh[e] = 0;
     float* stats = FIXED && sj.tile_stats ? sj.tile_stats + 4 * (size_t)tile : nullptr;
@@ -611,9 +621,19 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     float emax = 0.f, bmax = 0.f;
-    for (int r = threadIdx.x; r < 3 * V; r += blockDim.x) {
-      emax = fmaxf(emax, fabsf((float)Fs[r]));
-      bmax = fmaxf(bmax, fabsf((float)Fs[r + 3 * V]));
+    if (sizeof(R) == 4 && (3 * V) % 4 == 0) {     // 16-byte loads
+      const float4* e4 = reinterpret_cast<const float4*>(Fs);
+      const float4* b4 = e4 + (3 * V) / 4;
+      for (int r = threadIdx.x; r < (3 * V) / 4; r += blockDim.x) {
+        const float4 e = e4[r], b = b4[r];
+        emax = fmaxf(emax, fmaxf(fmaxf(fabsf(e.x), fabsf(e.y)), fmaxf(fabsf(e.z), fabsf(e.w))));
+        bmax = fmaxf(bmax, fmaxf(fmaxf(fabsf(b.x), fabsf(b.y)), fmaxf(fabsf(b.z), fabsf(b.w))));
+      }
+    } else {
+      for (int r = threadIdx.x; r < 3 * V; r += blockDim.x) {
+        emax = fmaxf(emax, fabsf((float)Fs[r]));
+        bmax = fmaxf(bmax, fabsf((float)Fs[r + 3 * V]));
+      }
     }
     emax = warp_max(emax); bmax = warp_max(bmax); umax2 = warp_max(umax2); wmax = warp_max(wmax);
     cmax = warp_max(cmax);
