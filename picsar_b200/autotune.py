@@ -53,8 +53,10 @@ def _cache_path():
     return os.path.join(os.path.expanduser("~"), ".cache", "picsar_b200", "autotune.json")
 
 
-def _key(order, precision, ppc, sigma, pusher, u_drift=0.0):
-    name = torch.cuda.get_device_name()
+def _key(order, precision, ppc, sigma, pusher, u_drift=0.0, device_name=None):
+    """Cache key of a job class: GPU model, order, precision, ppc, thermal
+    spread in half-decades, beam drift (2 decimals), pusher."""
+    name = device_name or torch.cuda.get_device_name()
     sb = round(math.log10(max(sigma, 1e-6)) * 2) / 2
     db = f"|d{round(u_drift, 2)}" if u_drift else ""
     return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}{db}|p{pusher}|v4"

@@ -5,7 +5,7 @@ import math
 
 import numpy as np
 
-from picsar_b200.autotune import proxy_grid, representative
+from picsar_b200.autotune import _key, proxy_grid, representative
 from picsar_b200.ensemble import JobSpec, ensemble_jobs, job_bytes
 from picsar_b200.serve import Request, fifo_latencies, percentile, poisson_requests
 
@@ -58,3 +58,12 @@ def test_autotune_representative_and_proxy():
     n = proxy_grid(8, 148)
     tiles = (n[0] // 8) * (n[1] // 8) * (n[2] // 8)
     assert tiles >= 2 * 148 * 2 and math.prod(n) * 8 <= 12_000_000
+
+
+def test_autotune_cache_keys():
+    k = lambda **kw: _key(**{**dict(order=3, precision="fp32", ppc=8, sigma=0.01, pusher=0,
+                                    device_name="GPU"), **kw})
+    assert k() == k(sigma=0.011)                       # same half-decade of spread
+    assert k() != k(sigma=0.05) and k() != k(ppc=16) and k() != k(order=2)
+    assert k() != k(u_drift=0.2) and k(u_drift=0.2) == k(u_drift=0.2001)
+    assert k().startswith("GPU|o3|fp32|ppc8|")
