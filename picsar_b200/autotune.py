@@ -1,16 +1,17 @@
 """Autotuner of the tiled engine: cell-tile shape (edge and window margin),
-threads per tile CTA and sort interval, chosen by timing.
+threads per tile CTA, sort interval and bank re-layout interval, chosen by
+timing.
 
-For a (shape order, precision, particles per cell, thermal spread) class of
-jobs, a proxy simulation large enough to occupy every SM (at least two tiles
+For a (shape order, precision, particles per cell, thermal spread, beam
+drift) class of jobs, a proxy simulation large enough to occupy every SM (at least two tiles
 per resident CTA) is stepped under each candidate and timed with CUDA events
 on the launching stream.  Stage 1 times every compiled (tile edge, margin)
 pair at both thread counts over 20 steps with a sort every 5 steps; stage 2
 times the two best at each pair of sort interval and bank re-layout interval
 over 40 steps (the slow path for particles that drifted out of their tile
 window, the bank conflicts of particles that changed cell, and the sorts
-and re-layouts themselves all count).  Results are cached per GPU model in a JSON file
-(``$PICSAR_B200_CACHE`` or ``~/.cache/picsar_b200/autotune.json``).
+and re-layouts themselves all count).  Results are cached per GPU model in
+a JSON file (``$PICSAR_B200_CACHE`` or ``~/.cache/picsar_b200/autotune.json``).
 
 The reference has no autotuner: its tile counts, vector lengths and
 sorting period are deck parameters (src/parallelization/tiling/tiling.F90,
