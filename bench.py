@@ -112,10 +112,11 @@ class ClockSampler:
 
     def __init__(self, dev_index):
         import torch
+        import tempfile
         self.proc = None
         self.index = None
-        os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_rank{dev_index}.csv")
+        fd, self.out = tempfile.mkstemp(prefix=f"pxrb_clocks_rank{dev_index}_", suffix=".csv")
+        os.close(fd)
         try:
             pr = torch.cuda.get_device_properties(dev_index)
             want = (int(pr.pci_domain_id), int(pr.pci_bus_id), int(pr.pci_device_id))
@@ -165,6 +166,10 @@ class ClockSampler:
                 for name, v in zip(self.NAMES, p[3:7]):
                     if v == "Active":
                         reasons.add(name)
+        try:
+            os.unlink(self.out)
+        except OSError:
+            pass
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),

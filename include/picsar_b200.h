@@ -30,12 +30,12 @@ extern "C" {
 #endif
 
 #define PXRB_OK 0
-#define PXRB_EINVAL 1
-#define PXRB_EUNSUPPORTED 2
-#define PXRB_ELAUNCH 3
-#define PXRB_ESCRATCH 4
-#define PXRB_ERANGE 5
-#define PXRB_ETOOLARGE 6
+#define PXRB_EINVAL 1        /* null pointer, negative or inconsistent size */
+#define PXRB_EUNSUPPORTED 2  /* shape order or option not implemented */
+#define PXRB_ELAUNCH 3       /* CUDA launch or runtime error */
+#define PXRB_ESCRATCH 4      /* caller's scratch buffer too small */
+#define PXRB_ERANGE 5        /* grid too small for its guard cells */
+#define PXRB_ETOOLARGE 6     /* job above the fixed limit of a no-allocation entry */
 
 /* ------------------------------------------------------------------------
  * Plain FP64 path (PICSAR arrays, one thread per particle, FP64 atomics)
@@ -357,11 +357,13 @@ int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* 
 /* Same diagnostics for callers that cannot allocate device memory (no
  * counterpart in the reference): the rho grid and the partial sums live in a
  * static device array owned by the library, so only the job and out (DEVICE
- * double[9]) are passed; gauss = 0 computes the energies only.  Jobs of more
- * than 1,048,576 cells are rejected with PXRB_ETOOLARGE.  Every GPU that loads
- * the library keeps the ~8.1 MiB array until exit; calls share it, so calls
- * that overlap on the GPU race.  The first call on a device looks up the
- * array's address (cudaGetSymbolAddress): make it before any stream capture. */
+ * double[9]) are passed; gauss = 0 computes the energies only (any job size).
+ * With gauss != 0, jobs of more than 1,048,576 cells are rejected with
+ * PXRB_ETOOLARGE.  Every GPU that loads the library keeps the ~8.1 MiB array
+ * until exit; calls share it, so calls that overlap on the GPU race.  The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress)
+ * and caches it for the process: make that call before any stream capture,
+ * and make no call after cudaDeviceReset (the cached address is then stale). */
 int pxrb_tiled_diagnostics_noalloc(const pxrb_tiled_job* job_host, int32_t gauss, double* out,
                                    void* stream);
 

@@ -17,7 +17,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libpxr_ref.so")
-REF_SRC = os.environ.get("PXR_REF_SRC", "/root/reference/src")
+# PICSAR src/ tree to translate; when unset, the oracle Makefile's default
+REF_SRC = os.environ.get("PXR_REF_SRC")
 _lib = None
 
 
@@ -34,9 +35,13 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            if not os.path.isdir(REF_SRC):
-                raise OSError("translated reference not built and reference sources absent")
-            subprocess.run(["make", "-C", _HERE, "-s", "ref", f"REF_SRC={REF_SRC}"], check=True)
+            cmd = ["make", "-C", _HERE, "-s", "ref-if-present"]
+            if REF_SRC:
+                cmd.append(f"REF_SRC={REF_SRC}")
+            subprocess.run(cmd, check=True)
+        if not os.path.exists(LIB_PATH):
+            raise OSError("translated reference not built and its sources absent "
+                          "(set PXR_REF_SRC to PICSAR's src/ tree)")
         _lib = C.CDLL(LIB_PATH)
     return _lib
 

@@ -10,17 +10,11 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-typedef int64_t i64;
+// The status codes (PXRB_OK, PXRB_EINVAL, ...) returned by every extern "C"
+// entry point are defined once, in the public header.
+#include "picsar_b200.h"
 
-// status codes returned by every extern "C" entry point
-enum {
-  PXRB_OK = 0,
-  PXRB_EINVAL = 1,       // null pointer, negative or inconsistent size
-  PXRB_EUNSUPPORTED = 2, // shape order / option not implemented
-  PXRB_ELAUNCH = 3,      // CUDA launch error (cudaGetLastError)
-  PXRB_ESCRATCH = 4,     // scratch buffer too small
-  PXRB_ERANGE = 5,       // grid too small for its guard cells
-};
+typedef int64_t i64;
 
 #define PXRB_CHECK_LAUNCH()                                  \
   do {                                                       \

@@ -767,8 +767,9 @@ int pxrb_depose_rho(int64_t order, double* rho, int64_t np, const double* xp,
 
 static GridG grid_lohi(const int64_t* lo, const int64_t* hi) {
   GridG g;
-  // represent (lo:hi) as n = hi + lo... use guards = -lo, n = hi - lo + lo... :
-  // idx(i) = (i - lo) + ...; with gx = -lo and nx = hi + lo (so nx + 2gx = hi - lo)
+  // An array with Fortran bounds (lo:hi) per axis as a guarded grid: guards
+  // gx = -lo, so that idx(i) = i - lo; and nx = hi + lo, so that the extent
+  // nx + 1 + 2 gx equals hi - lo + 1.
   g.gx = -lo[0]; g.gy = -lo[1]; g.gz = -lo[2];
   g.nx = hi[0] + lo[0]; g.ny = hi[1] + lo[1]; g.nz = hi[2] + lo[2];
   g.sx = hi[0] - lo[0] + 1;

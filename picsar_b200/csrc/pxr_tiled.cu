@@ -728,10 +728,13 @@ __global__ void __launch_bounds__(288) k_diag_final(Job J, const double* part, i
   }
 }
 
+// blocks of the diagnostics reduction: at most DIAG_MAX_BLOCKS (8 per SM of
+// a B200), each writing 9 partial sums
+constexpr int DIAG_MAX_BLOCKS = 1184;
 int diag_blocks(const Job& J) {
   i64 total = (i64)J.nx * J.ny * J.nz;
   i64 b = (total + RED_TPB - 1) / RED_TPB;
-  return (int)(b > 1184 ? 1184 : (b < 1 ? 1 : b));
+  return (int)(b > DIAG_MAX_BLOCKS ? DIAG_MAX_BLOCKS : (b < 1 ? 1 : b));
 }
 
 template <int ORDER>
@@ -1001,19 +1004,24 @@ int pxrb_tiled_diagnostics(const pxrb_tiled_job* job_host, double* rho, double* 
 // the caller passes nothing but the job and the 9-double output.
 //
 // Limits and rules:
-//  * the array holds PXRB_NOALLOC_RHO_MAX doubles of rho (jobs of at most
-//    1,048,576 cells, e.g. 96^3 or 128x128x64) plus the partial sums; larger
-//    jobs are rejected with PXRB_ETOOLARGE before any GPU work;
+//  * the array holds PXRB_NOALLOC_RHO_MAX doubles of rho (with gauss != 0,
+//    jobs of at most 1,048,576 cells, e.g. 96^3 or 128x128x64) plus the
+//    partial sums of the reduction, whose block count is capped, so jobs of
+//    any size fit with gauss = 0; a larger job with gauss != 0 is rejected
+//    with PXRB_ETOOLARGE before any GPU work;
 //  * every GPU that loads the library holds the array (~8.1 MiB) until exit;
 //  * every call shares the array and it keeps the last call's contents, so
 //    calls that overlap on the GPU (different streams, or a second call
 //    enqueued before the first finished, from any thread) race;
 //  * the first call on a device resolves the array's device address with
 //    cudaGetSymbolAddress (once per device); make that first call before any
-//    stream capture.
+//    stream capture;
+//  * that address is cached per device index for the life of the process: it
+//    does not survive cudaDeviceReset (or any other teardown of the device's
+//    primary context), after which this entry point must not be called.
 // ---------------------------------------------------------------------------
 #define PXRB_NOALLOC_RHO_MAX (1 << 20)
-#define PXRB_NOALLOC_PART_MAX (9 * 1184)
+#define PXRB_NOALLOC_PART_MAX (9 * DIAG_MAX_BLOCKS)
 static __device__ __align__(256) double g_noalloc_scratch[PXRB_NOALLOC_RHO_MAX + PXRB_NOALLOC_PART_MAX];
 
 static std::mutex g_noalloc_mu;
@@ -1024,8 +1032,9 @@ extern "C" int pxrb_tiled_diagnostics_noalloc(const pxrb_tiled_job* job_host, in
   if (!job_host || !out) return PXRB_EINVAL;
   const Job& J = *job_host;
   const i64 ncell = (i64)J.nx * J.ny * J.nz;
-  const int nb = diag_blocks(J);
-  if (ncell > PXRB_NOALLOC_RHO_MAX || 9 * nb > PXRB_NOALLOC_PART_MAX) return PXRB_ETOOLARGE;
+  static_assert(PXRB_NOALLOC_PART_MAX >= 9 * DIAG_MAX_BLOCKS,
+                "the partial sums of the largest reduction must fit the static array");
+  if (gauss && ncell > PXRB_NOALLOC_RHO_MAX) return PXRB_ETOOLARGE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return PXRB_ELAUNCH;
   double* base = nullptr;

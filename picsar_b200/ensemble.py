@@ -52,6 +52,12 @@ class JobSpec:
     steps: int = 100
     seed: int = 0
 
+    def __post_init__(self):
+        if int(self.steps) < 1:
+            raise ValueError(f"a job runs at least one step (steps = {self.steps})")
+        if int(self.ppc) < 0 or min(int(v) for v in self.n) < 1:
+            raise ValueError(f"invalid job size: n = {self.n}, ppc = {self.ppc}")
+
     @property
     def cells(self) -> int:
         return int(self.n[0]) * int(self.n[1]) * int(self.n[2])

@@ -67,3 +67,12 @@ def test_autotune_cache_keys():
     assert k() != k(sigma=0.05) and k() != k(ppc=16) and k() != k(order=2)
     assert k() != k(u_drift=0.2) and k(u_drift=0.2) == k(u_drift=0.2001)
     assert k().startswith("GPU|o3|fp32|ppc8|")
+
+
+def test_job_spec_rejects_jobs_without_steps():
+    import pytest
+    for bad in (0, -3):
+        with pytest.raises(ValueError, match="at least one step"):
+            JobSpec(n=(16, 16, 16), ppc=1, sigma=0.01, order=1, steps=bad)
+    with pytest.raises(ValueError):
+        JobSpec(n=(16, 0, 16), ppc=1, sigma=0.01, order=1)

@@ -54,3 +54,20 @@ def test_noalloc_rejects_jobs_above_its_limit(cuda):
     t = TiledSim((128, 128, 72), order=1, precision="fp32", config=TiledConfig(tile=(8, 8, 8)))
     with pytest.raises(PicsarB200Error, match="status 6"):
         t.diagnostics_noalloc(gauss=True)
+
+
+def test_noalloc_energies_of_a_job_above_the_rho_limit(cuda):
+    # without the Gauss residual no rho grid is needed: any job size is served
+    from picsar_b200 import picsar as P
+    n, g = (128, 128, 72), 3
+    st = thermal_plasma(n, 1, 0.02, seed=33)
+    t = TiledSim(n, order=1, precision="fp32", config=TiledConfig(tile=(8, 8, 8)))
+    for name, a in zip(("ex", "ey", "ez", "bx", "by", "bz"), random_fields(n, g, seed=34)):
+        t.import_field(name, P.to_fortran(a), g)
+    t.load_state(st.to(device="cuda"))
+    t.step(1)
+    for _ in range(2):
+        ref = t.diagnostics(gauss=False)
+        got = t.diagnostics_noalloc(gauss=False)
+        for k in ("kinetic", "ex", "ey", "ez", "bx", "by", "bz"):
+            assert _close(got[k], ref[k]), (k, got[k], ref[k])
