@@ -347,6 +347,7 @@ def run_ours(args):
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
     launches0 = sim.launches
+    deferred0 = sim.deferred_count()
     _barrier(ws)
     clocks.start()
     t_start.record(stream)
@@ -359,6 +360,7 @@ def run_ours(args):
     ms_total = _max_over_ranks(ms_total, ws)
     kern_ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
     launches = sim.launches - launches0
+    deferred = (sim.deferred_count() - deferred0) / (N * args.steps)
     e1 = sim.diagnostics(gauss=False)
     slow = sim.slow_path_count()
     value = N * ws * args.steps / (ms_total * 1e-3)
@@ -435,6 +437,7 @@ def run_ours(args):
             "energy": {"start": e0["total"], "end": e1["total"],
                        "rel_change": (e1["total"] - e0["total"]) / e0["total"]},
             "slow_path_particle_steps": slow,
+            "deferred_fraction": deferred,
             "accuracy": accuracy,
         }
         print(json.dumps(line), flush=True)

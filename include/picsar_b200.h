@@ -219,7 +219,9 @@ typedef struct pxrb_tiled_job {
   int32_t* tile_cnt;                        /* ntiles + 1 (sort scratch) */
   double* ke_tile;                          /* ntiles: kinetic energy per tile */
   int32_t* counters;                        /* [0] particles on the slow path,
-                                               [1] error flag */
+                                               [1] error flag, [2] particles the FP32
+                                               kernel deferred to its second pass
+                                               (bank classes taken); int32[4] */
   int32_t* cell_cnt;                        /* sort scratch: ntiles * tile^3 */
   int32_t* rank_b;                          /* sort scratch: np */
   int32_t* perm;                            /* sort scratch: np */

@@ -271,8 +271,18 @@ template <> struct Acc<0> {
 template <> struct Acc<1> {
   typedef int T;
   static constexpr int NW = 1;
-  static constexpr double SCALE_BITS = 536870912.0;   // 2^29
-  __device__ __forceinline__ static void add(int* p, float v, int) { atomicAdd(p, __float2int_rn(v)); }
+  static constexpr double SCALE_BITS = 536870912.0;   // 2^29 (2^28 at order 1, below)
+  // v rounded to the nearest integer by adding 1.5 * 2^23: for |v| <= 2^22
+  // the sum lies in [2^23, 2^24], where the float spacing is 1, so its low
+  // mantissa bits are round(v) + 2^22 (round half to even, as
+  // __float2int_rn).  One FADD and one integer subtract replace a
+  // conversion instruction, which issues at a fraction of the FMA rate.
+  // The scale keeps every contribution within 2^22: it is at most
+  // SCALE_BITS / (L+H+3)^3, i.e. 2^28 / 64 at order 1 and 2^29 / 216 above.
+  __device__ __forceinline__ static void add(int* p, float v, int) {
+    const float t = v + 12582912.0f;
+    atomicAdd(p, __float_as_int(t) - 0x4B400000);
+  }
   __device__ __forceinline__ static double get(const int* p, int r, int) { return (double)p[r]; }
 };
 template <> struct Acc<2> {
@@ -468,7 +478,89 @@ __device__ __forceinline__ R gwin(const R* base, const R* sa, const R* sb, const
   return out;
 }
 
+// Fixed-point resolution of a mode: the largest node sum, as an integer.
+template <int MODE, int ORDER> __host__ __device__ constexpr double scale_bits() {
+  return (MODE == 1 && ORDER == 1) ? 268435456.0 : Acc<MODE>::SCALE_BITS;   // 2^28
+}
+
+// ---------------------------------------------------------------------------
+// Packed FP32 pairs (sm_100 fma/mul .f32x2): one instruction performs two
+// independent single-precision operations, each rounded as its scalar form.
+// ---------------------------------------------------------------------------
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t f2_pack(float lo, float hi) {
+  f2_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float f2_sum(f2_t v) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+  return lo + hi;
+}
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+  f2_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
+  f2_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// FP32 window gather with the z-planes taken in pairs: each packed FMA
+// advances two planes' sums, so the point sums of a component take
+// NA*NB*ceil(NC/2) instructions instead of NA*NB*NC.  An odd last plane is
+// summed in scalar form.  The per-plane sums are those of gwin; only the
+// final sum over the planes is ordered differently.
+template <int NA, int NB, int NC, int SY, int SZ>
+__device__ __forceinline__ float gwin2(const float* base, const f2_t* sa2, const f2_t* sb2,
+                                       const float* sc) {
+  f2_t out2 = f2_pack(0.f, 0.f);
+#pragma unroll
+  for (int c = 0; c + 1 < NC; c += 2) {
+    f2_t a2;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      f2_t r2 = f2_mul(f2_pack(base[b * SY + c * SZ], base[b * SY + (c + 1) * SZ]), sa2[0]);
+#pragma unroll
+      for (int t = 1; t < NA; ++t)
+        r2 = f2_fma(f2_pack(base[t + b * SY + c * SZ], base[t + b * SY + (c + 1) * SZ]), sa2[t], r2);
+      a2 = b == 0 ? f2_mul(r2, sb2[0]) : f2_fma(r2, sb2[b], a2);
+    }
+    out2 = f2_fma(a2, f2_pack(sc[c], sc[c + 1]), out2);
+  }
+  float out = f2_sum(out2);
+  if (NC & 1) {
+    constexpr int c = NC - 1;
+    float a = 0.f;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      float r = 0.f;
+#pragma unroll
+      for (int t = 0; t < NA; ++t) {
+        float sat, dummy;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(sat), "=f"(dummy) : "l"(sa2[t]));
+        r = r + sat * base[t + b * SY + c * SZ];
+      }
+      float sbb, dummy2;
+      asm("mov.b64 {%0, %1}, %2;" : "=f"(sbb), "=f"(dummy2) : "l"(sb2[b]));
+      a = a + r * sbb;
+    }
+    out = out + a * sc[c];
+  }
+  return out;
+}
+
+template <int N>
+__device__ __forceinline__ void f2_splat(const float* s, f2_t* s2) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) s2[i] = f2_pack(s[i], s[i]);
+}
+
 constexpr int MAX_THREADS = 256;
+
 // Window particles whose Esirkepov node changes along some axis are queued
 // and deposited after the tile's main loop by full warps, so the common
 // same-node path never diverges into the general one.  The queue lives in
@@ -508,6 +600,10 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
   __shared__ Job sj;
   __shared__ int s_item;
   __shared__ int s_qn;
+  // bank-conflict-free pass selection (FP32 windows; see the particle loop)
+  constexpr bool SELECT = sizeof(R) == 4;
+  __shared__ int s_dn;                             // deferred particles of the tile
+  __shared__ int s_dcnt[32];                       // ... per bank class
   __shared__ float s_max[5][MAX_THREADS / 32];
   __shared__ double s_red[MAX_THREADS / 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -523,6 +619,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     if (threadIdx.x == 0) {
       s_item = atomicAdd(ctr, 1);
       s_qn = 0;
+      s_dn = 0;
     }
     __syncthreads();
     const int item = s_item;
@@ -662,7 +759,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
         const double dq = q == 0 ? sj.dx : (q == 1 ? sj.dy : sj.dz);
         const double disp = fmin(vb * sj.dt / dq, 1.0);
         const double bound = fabs(sj.q) * (double)Wm * dq / (sj.dt * dV) * disp;
-        const double s = Acc<MODE>::SCALE_BITS / fmax(np_ * bound, 1e-300);
+        const double s = scale_bits<MODE, ORDER>() / fmax(np_ * bound, 1e-300);
         scale[q] = fmin(s, 1e30);
       }
     }
@@ -687,7 +784,31 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     int nslow = 0, bad = 0;
     __syncthreads();
 
-    for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
+    // Two passes over the tile.  Pass 0 takes the particles in storage
+    // order, 32 consecutive ones per warp; a window particle whose bank class
+    // (the bank of its stencil origin in the window, so of every one of its
+    // gather loads and fast-path atomics) a lower lane of the warp already
+    // holds is deferred, so every warp instruction of the pass reads or
+    // updates 32 distinct banks whatever the particles' drift since the last
+    // sort.  Pass 1 takes the deferred particles bucketed by class, in
+    // (rank, class) order, so its warps too hold distinct classes except at
+    // the tail.  FP32 windows only (one 4-byte bank per element); the FP64
+    // engine makes one pass.  The deferred list, its classes and its
+    // bucketed order live in the tile's range of sort scratch that is free
+    // between sorts: perm, and ux_b / uy_b / uz_b taken as integers.
+    int* d_list = sj.perm;
+    int* d_ord = reinterpret_cast<int*>(sj.ux_b);
+    int* d_rank = reinterpret_cast<int*>(sj.uy_b);
+    int* d_key = reinterpret_cast<int*>(sj.uz_b);
+#pragma unroll 1
+    for (int phase = 0; phase < (SELECT ? 2 : 1); ++phase) {
+    const int cnt = phase == 0 ? pend - pbeg : s_dn;
+    for (int s0 = threadIdx.x & ~31; s0 < cnt; s0 += blockDim.x) {
+      const int sl = s0 + lane;
+      const bool valid = sl < cnt;
+      // lanes past the end read a valid particle and do nothing with it
+      const int slc = valid ? sl : 0;
+      const int ip = phase == 0 ? pbeg + slc : d_list[pbeg + d_ord[pbeg + slc]];
       int ci, cj, ck;
       unpack_cell(cellp[ip], ci, cj, ck);
       const R ox = oxp[ip], oy = oyp[ip], oz = ozp[ip];
@@ -699,6 +820,26 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       if (vz > tez - 1 + D) vz -= nz; else if (vz < -D) vz += nz;
       const bool in_old = vx >= -D && vx <= tex - 1 + D && vy >= -D && vy <= tey - 1 + D &&
                           vz >= -D && vz <= tez - 1 + D;
+      if (SELECT && phase == 0) {
+        const bool part = valid && in_old;
+        const int hx = ORDER == 2 && ox >= (R)0.5, hy = ORDER == 2 && oy >= (R)0.5,
+                  hz = ORDER == 2 && oz >= (R)0.5;
+        const int key = (vx + hx + (vy + hy) * SY + (vz + hz) * SZ + (D + L) * (1 + SY + SZ)) & 31;
+        // lanes holding the same class: five ballots over the class bits
+        unsigned peers = __ballot_sync(0xffffffffu, part);
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {
+          const unsigned m = __ballot_sync(0xffffffffu, part && ((key >> b) & 1));
+          peers &= ((key >> b) & 1) ? m : ~m;
+        }
+        if (part && (peers & ((1u << lane) - 1u))) {
+          const int q = atomicAdd(&s_dn, 1);
+          d_list[pbeg + q] = ip;
+          d_key[pbeg + q] = key;
+          continue;
+        }
+      }
+      if (!valid) continue;
       // ---- gather ----------------------------------------------------------
       R eb[6];
       if (in_old) {
@@ -709,12 +850,26 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
         sxs.set(ox); sys.set(oy); szs.set(oz);
         constexpr int N = ORDER + 1, S = ORDER;
         const R* F0 = Fs + wx + wy * SY + wz * SZ;
-        eb[0] = gwin<S, N, N, SY, SZ>(F0 + sxs.r0 + nys.r0 * SY + nzs.r0 * SZ, sxs.s, nys.s, nzs.s);
-        eb[1] = gwin<N, S, N, SY, SZ>(F0 + V + nxs.r0 + sys.r0 * SY + nzs.r0 * SZ, nxs.s, sys.s, nzs.s);
-        eb[2] = gwin<N, N, S, SY, SZ>(F0 + 2 * V + nxs.r0 + nys.r0 * SY + szs.r0 * SZ, nxs.s, nys.s, szs.s);
-        eb[3] = gwin<N, S, S, SY, SZ>(F0 + 3 * V + nxs.r0 + sys.r0 * SY + szs.r0 * SZ, nxs.s, sys.s, szs.s);
-        eb[4] = gwin<S, N, S, SY, SZ>(F0 + 4 * V + sxs.r0 + nys.r0 * SY + szs.r0 * SZ, sxs.s, nys.s, szs.s);
-        eb[5] = gwin<S, S, N, SY, SZ>(F0 + 5 * V + sxs.r0 + sys.r0 * SY + nzs.r0 * SZ, sxs.s, sys.s, nzs.s);
+        if constexpr (sizeof(R) == 4 && ORDER > 1) {
+          // x and y shapes splatted once into packed pairs for the z-plane pairs
+          f2_t nx2[N], sx2[S], ny2[N], sy2[S];
+          f2_splat<N>((const float*)nxs.s, nx2); f2_splat<S>((const float*)sxs.s, sx2);
+          f2_splat<N>((const float*)nys.s, ny2); f2_splat<S>((const float*)sys.s, sy2);
+          const float* Ff = (const float*)F0;
+          eb[0] = gwin2<S, N, N, SY, SZ>(Ff + sxs.r0 + nys.r0 * SY + nzs.r0 * SZ, sx2, ny2, (const float*)nzs.s);
+          eb[1] = gwin2<N, S, N, SY, SZ>(Ff + V + nxs.r0 + sys.r0 * SY + nzs.r0 * SZ, nx2, sy2, (const float*)nzs.s);
+          eb[2] = gwin2<N, N, S, SY, SZ>(Ff + 2 * V + nxs.r0 + nys.r0 * SY + szs.r0 * SZ, nx2, ny2, (const float*)szs.s);
+          eb[3] = gwin2<N, S, S, SY, SZ>(Ff + 3 * V + nxs.r0 + sys.r0 * SY + szs.r0 * SZ, nx2, sy2, (const float*)szs.s);
+          eb[4] = gwin2<S, N, S, SY, SZ>(Ff + 4 * V + sxs.r0 + nys.r0 * SY + szs.r0 * SZ, sx2, ny2, (const float*)szs.s);
+          eb[5] = gwin2<S, S, N, SY, SZ>(Ff + 5 * V + sxs.r0 + sys.r0 * SY + nzs.r0 * SZ, sx2, sy2, (const float*)nzs.s);
+        } else {
+          eb[0] = gwin<S, N, N, SY, SZ>(F0 + sxs.r0 + nys.r0 * SY + nzs.r0 * SZ, sxs.s, nys.s, nzs.s);
+          eb[1] = gwin<N, S, N, SY, SZ>(F0 + V + nxs.r0 + sys.r0 * SY + nzs.r0 * SZ, nxs.s, sys.s, nzs.s);
+          eb[2] = gwin<N, N, S, SY, SZ>(F0 + 2 * V + nxs.r0 + nys.r0 * SY + szs.r0 * SZ, nxs.s, nys.s, szs.s);
+          eb[3] = gwin<N, S, S, SY, SZ>(F0 + 3 * V + nxs.r0 + sys.r0 * SY + szs.r0 * SZ, nxs.s, sys.s, szs.s);
+          eb[4] = gwin<S, N, S, SY, SZ>(F0 + 4 * V + sxs.r0 + nys.r0 * SY + szs.r0 * SZ, sxs.s, nys.s, szs.s);
+          eb[5] = gwin<S, S, N, SY, SZ>(F0 + 5 * V + sxs.r0 + sys.r0 * SY + nzs.r0 * SZ, sxs.s, sys.s, nzs.s);
+        }
       } else {
         gather_global<ORDER, R>(sj, ci, cj, ck, ox, oy, oz, eb);
       }
@@ -809,6 +964,28 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       }
     }
     __syncthreads();
+    if (SELECT && phase == 0 && s_dn > 0) {
+      // bucket the deferred particles by class: the entry of rank r in class
+      // k goes to sum_c min(n_c, r) + #{c < k : n_c > r}
+      const int nd = s_dn;
+      if (threadIdx.x < 32) s_dcnt[threadIdx.x] = 0;
+      __syncthreads();
+      for (int q = threadIdx.x; q < nd; q += blockDim.x)
+        d_rank[pbeg + q] = atomicAdd(&s_dcnt[d_key[pbeg + q]], 1);
+      __syncthreads();
+      for (int q = threadIdx.x; q < nd; q += blockDim.x) {
+        const int k = d_key[pbeg + q], r = d_rank[pbeg + q];
+        int P = 0;
+#pragma unroll 8
+        for (int c = 0; c < 32; ++c) {
+          const int n = s_dcnt[c];
+          P += min(n, r) + (c < k && n > r ? 1 : 0);
+        }
+        d_ord[pbeg + P] = q;
+      }
+      __syncthreads();
+    }
+    }   // phase
     // ---- deferred window particles with a node change ------------------------
     {
       const int nq = s_qn;
@@ -860,6 +1037,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       if (lane == 0) s_red[wid] = v;
       if (nslow) atomicAdd(&sj.counters[0], nslow);
       if (bad) atomicExch(&sj.counters[1], 1);
+      if (SELECT && threadIdx.x == 0 && s_dn) atomicAdd(&sj.counters[2], s_dn);
       if (FIXED && stats) {
         float c = 0.f;
         for (int r = threadIdx.x; r < HB * HB * HB; r += blockDim.x) c = fmaxf(c, (float)nh[r]);

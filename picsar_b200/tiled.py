@@ -384,6 +384,11 @@ class TiledSim:
     def error_flag(self):
         return int(self.counters[1].item())
 
+    def deferred_count(self):
+        """Particle-steps the FP32 particle kernel deferred to its second,
+        class-bucketed pass since the simulation was created."""
+        return int(self.counters[2].item())
+
     def particles(self):
         """PICSAR-style FP64 particle arrays (sorted by id when ids are tracked)."""
         self._pull_job()
