@@ -179,6 +179,22 @@ int pxrb_particle_bcs_periodic(int64_t np, double* xp, double* yp, double* zp, d
                                double ymin, double zmin, double xmax, double ymax,
                                double zmax, void* stream);
 
+/* Replaces pxr_particle_bin_sorting (src/housekeeping/sorting.F90:247-361):
+ * particles reordered by bin number iz*nx3*ny3 + iy*nx3 + ix, with
+ * (ix, iy, iz) = floor((x - xmin2) / dxf, ...) and nx3 = ceil((xmax2 - xmin2)
+ * / dxf) ..., keeping the input order inside a bin (the reference's counting
+ * sort is stable).  Positions outside [min2, max2) go to the nearest end bin
+ * (the reference checks this only in DEBUG builds).  xp..gam are permuted in
+ * place, and w (the pid weight column, the only pid column the reference
+ * carries along, sorting.F90:264) when not NULL.  scratch: DEVICE bytes,
+ * scratch_bytes >= pxrb_particle_bin_sorting_scratch(np); np < 2^31. */
+int64_t pxrb_particle_bin_sorting_scratch(int64_t np);
+int pxrb_particle_bin_sorting(int64_t np, double* xp, double* yp, double* zp, double* ux,
+                              double* uy, double* uz, double* gam, double* w, double xmin2,
+                              double ymin2, double zmin2, double xmax2, double ymax2,
+                              double zmax2, double dxf, double dyf, double dzf, void* scratch,
+                              int64_t scratch_bytes, void* stream);
+
 
 /* ------------------------------------------------------------------------
  * Tiled engine (B200-native layout): FP32 mixed precision or FP64.

@@ -98,6 +98,7 @@ def _declare(L):
     L.orc_sim_diags.argtypes = [vp, P]
     L.orc_sim_phase.argtypes = [vp, i64]
     L.orc_num_threads.restype = C.c_int
+    L.orc_particle_bin_sorting.argtypes = [i64] + [P] * 8 + [f64] * 9
 
 
 def _c(a):
@@ -130,6 +131,12 @@ def set_gamma(ux, uy, uz, gaminv, clight=1.0):
 
 def pushxyz(x, y, z, ux, uy, uz, gaminv, dt):
     lib().orc_pushxyz(len(x), _p(x), _p(y), _p(z), _p(ux), _p(uy), _p(uz), _p(gaminv), dt)
+
+
+def particle_bin_sorting(x, y, z, ux, uy, uz, gam, w, lo, hi, dbin):
+    """pxr_particle_bin_sorting on flat float64 arrays, in place; w may be None."""
+    lib().orc_particle_bin_sorting(len(x), _p(x), _p(y), _p(z), _p(ux), _p(uy), _p(uz),
+                                   _p(gam), None if w is None else _p(w), *lo, *hi, *dbin)
 
 
 def ebcancelpush3d(ux, uy, uz, gi, ex, ey, ez, bx, by, bz, q, m, dt, which, clight=1.0):

@@ -479,6 +479,51 @@ void orc_field_gathering_plus_particle_pusher_3_3_3(
   }
 }
 
+// pxr_particle_bin_sorting (src/housekeeping/sorting.F90:247-361) on one set
+// of flat arrays: bin id iz*nx3*ny3 + iy*nx3 + ix + 1 from floor((x - xmin2) *
+// dxi), counts per bin, exclusive prefix, then each particle in input order
+// to the next slot of its bin; the weight column w (may be NULL) travels with
+// the particles.  Bins outside the range (a DEBUG-only STOP in the reference)
+// are clamped to the nearest end bin.
+void orc_particle_bin_sorting(i64 np2, double* xp, double* yp, double* zp, double* ux,
+                              double* uy, double* uz, double* gam, double* w, double xmin2,
+                              double ymin2, double zmin2, double xmax2, double ymax2,
+                              double zmax2, double dxf, double dyf, double dzf) {
+  const double dxi = 1. / dxf, dyi = 1. / dyf, dzi = 1. / dzf;
+  const i64 nx3 = (i64)std::ceil((xmax2 - xmin2) * dxi);
+  const i64 ny3 = (i64)std::ceil((ymax2 - ymin2) * dyi);
+  const i64 nz3 = (i64)std::ceil((zmax2 - zmin2) * dzi);
+  const i64 nbhc = nx3 * ny3 * nz3;
+  std::vector<i64> hcnb(np2), piihc(nbhc + 1, 0), nbppc(nbhc + 1, 0);
+  for (i64 ip = 0; ip < np2; ++ip) {
+    const double x2 = (xp[ip] - xmin2) * dxi, y2 = (yp[ip] - ymin2) * dyi,
+                 z2 = (zp[ip] - zmin2) * dzi;
+    const i64 ix = ffloor(x2), iy = ffloor(y2), iz = ffloor(z2);
+    i64 h = iz * nx3 * ny3 + iy * nx3 + ix + 1;
+    h = h < 1 ? 1 : (h > nbhc ? nbhc : h);
+    hcnb[ip] = h;
+    nbppc[h] = nbppc[h] + 1;
+  }
+  i64 k = 0;
+  for (i64 ic = 1; ic <= nbhc; ++ic) {
+    piihc[ic] = k;
+    k = k + nbppc[ic];
+  }
+  std::vector<i64> dest(np2);
+  for (i64 ip = 0; ip < np2; ++ip) {
+    const i64 kk = hcnb[ip];
+    piihc[kk] = piihc[kk] + 1;
+    dest[ip] = piihc[kk] - 1;              // 1-based slot piihc(k) -> 0-based
+  }
+  double* cols[8] = {xp, yp, zp, ux, uy, uz, gam, w};
+  std::vector<double> tmp(np2);
+  for (double* c : cols) {
+    if (!c) continue;
+    for (i64 ip = 0; ip < np2; ++ip) tmp[dest[ip]] = c[ip];
+    std::copy(tmp.begin(), tmp.end(), c);
+  }
+}
+
 }  // extern "C"
 
 // ----------------------------------------------------------------------------

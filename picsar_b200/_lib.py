@@ -45,6 +45,8 @@ _SIGS = {
     "pxrb_field_bc_periodic": "p p p" + " i" * 6 + " s",
     "pxrb_summation_bcs_periodic": "p p p" + " i" * 6 + " s",
     "pxrb_particle_bcs_periodic": "i p p p" + " d" * 6 + " s",
+    "pxrb_particle_bin_sorting": "i" + " p" * 8 + " d" * 9 + " p i s",
+    "pxrb_particle_bin_sorting_scratch": "=i i",
 }
 for _o in (1, 2, 3):
     _SIGS[f"pxrb_field_gathering_plus_particle_pusher_{_o}_{_o}_{_o}"] = (

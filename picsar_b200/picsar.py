@@ -15,10 +15,24 @@ Two layers, both named after the reference:
 
 * ``PicsarModule``: module variables (``nx``, ``dt``, ``ex`` ... ) and the
   global drivers acting on them (``field_gathering_plus_particle_pusher``,
-  ``particle_bcs``, ``pxrdepose_currents_on_grid_jxjyjz``, ``current_bcs``,
-  ``push_bfield``, ``bfield_bcs``, ``push_efield``, ``efield_bcs``,
-  ``calc_diags``, ``step``), the plain FP64 GPU path of the step loop of
-  src/submain.F90:104-195.
+  ``particle_bcs``, ``pxr_particle_sorting``,
+  ``pxrdepose_currents_on_grid_jxjyjz``, ``current_bcs``, ``push_bfield``,
+  ``bfield_bcs``, ``push_efield``, ``efield_bcs``, ``calc_diags``, ``step``),
+  the step loop of src/submain.F90:104-195, on one of two engines:
+
+  - ``engine="plain"``: PICSAR's own arrays in FP64, one kernel per routine
+    (the comparison baseline);
+  - ``engine="tiled"``: the B200 tiled engine (``picsar_b200.tiled``) in FP64
+    or FP32 mixed precision.  The state lives in the engine's layout; the
+    module arrays and the species' ``part_*`` arrays are PICSAR-layout FP64
+    views filled when they are read, and a view that was handed out is
+    written back into the engine before the next engine operation, so code
+    that reads or edits module arrays between driver calls sees the
+    reference's behaviour.  Gather, push, periodic wrap and deposition are
+    one fused kernel, launched by ``field_gathering_plus_particle_pusher``;
+    ``pxrdepose_currents_on_grid_jxjyjz`` then finds J deposited, and the
+    boundary routines have nothing left to do (the engine writes periodic
+    guards itself).
 """
 from __future__ import annotations
 
@@ -127,12 +141,41 @@ class Species:
         return 0 if self.part_x is None else int(self.part_x.numel())
 
 
+_GRIDS = ("ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz", "rho", "dive")
+
+
+def _grid_property(name):
+    def get(self):
+        if self._tiled is not None:
+            return self._tiled.grid(name)
+        return self._grids[name]
+
+    def set_(self, value):
+        if self._tiled is not None:
+            self._tiled.set_grid(name, value)
+        else:
+            self._grids[name] = value
+    return property(get, set_, doc=f"module array {name} (PICSAR layout, FP64)")
+
+
 class PicsarModule:
-    """Module variables and global drivers of the plain FP64 GPU path."""
+    """Module variables and global drivers of PICSAR's step loop.
+
+    engine: "plain" (PICSAR arrays, FP64) or "tiled" (the B200 tiled engine;
+    precision "fp64" or "fp32" mixed, tuning ``tiled_config``, one pushed
+    species)."""
 
     def __init__(self, nx, ny, nz, nguards=3, dx=1.0, dy=1.0, dz=1.0, xmin=0.0, ymin=0.0,
                  zmin=0.0, dtcoef=0.95, dt=None, nox=1, particle_pusher=0, clight=1.0,
-                 mu0=1.0, eps0=1.0, device="cuda"):
+                 mu0=1.0, eps0=1.0, device="cuda", engine="plain", precision="fp64",
+                 tiled_config=None):
+        if engine not in ("plain", "tiled"):
+            raise ValueError("engine must be 'plain' or 'tiled'")
+        if engine == "plain" and precision != "fp64":
+            raise ValueError("the plain engine computes in FP64 only")
+        self._tiled = None
+        self._grids = {}
+        self.engine, self.precision = engine, precision
         self.device = torch.device(device)
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.nxguards = self.nyguards = self.nzguards = int(nguards)
@@ -153,17 +196,30 @@ class PicsarModule:
         self.l_lower_order_in_v = True
         self.currdepo = 0
         self.it = 0
-        g = self.nxguards
-        mk = lambda: grid_zeros(self.nx, self.ny, self.nz, g, device=self.device)
-        self.ex, self.ey, self.ez = mk(), mk(), mk()
-        self.bx, self.by, self.bz = mk(), mk(), mk()
-        self.jx, self.jy, self.jz = mk(), mk(), mk()
-        self.rho, self.dive = mk(), mk()
+        # particle sorting (shared_data, modules.F90:1491-1503): off by default
+        # (control_file.F90:160-166); bin sizes in physical units, as after
+        # the scaling by dx at start-up (submain.F90:601)
+        self.sorting_activated = 0
+        self.sorting_dx, self.sorting_dy, self.sorting_dz = self.dx, self.dy, self.dz
+        self.sorting_shiftx = self.sorting_shifty = self.sorting_shiftz = 0.0
+        self._sort_scratch = None
         self.species = []
         self._err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        g = self.nxguards
+        if engine == "tiled":
+            self._tiled = _TiledState(self, precision, tiled_config)
+        else:
+            for name in _GRIDS:
+                self._grids[name] = grid_zeros(self.nx, self.ny, self.nz, g, device=self.device)
 
     # -- particles ----------------------------------------------------------
-    def add_species(self, name, charge, mass, x, y, z, ux, uy, uz, w, pid=None):
+    def add_species(self, name, charge, mass, x, y, z, ux, uy, uz, w, pid=None,
+                    sorting_period=0, sorting_start=0):
+        if self._tiled is not None:
+            sp = self._tiled.add_species(name, charge, mass, x, y, z, ux, uy, uz, w, pid)
+            sp.sorting_period, sp.sorting_start = int(sorting_period), int(sorting_start)
+            self.species.append(sp)
+            return sp
         dev, f = self.device, torch.float64
         t = lambda a: torch.as_tensor(a, dtype=f).to(dev).contiguous()
         sp = Species(name, float(charge), float(mass))
@@ -176,13 +232,18 @@ class PicsarModule:
             setattr(sp, "part_" + c, torch.zeros(n, dtype=f, device=dev))
         sp.pid_w = t(w)
         sp.pid_id = t(pid) if pid is not None else torch.arange(n, dtype=f, device=dev)
+        sp.sorting_period, sp.sorting_start = int(sorting_period), int(sorting_start)
         self.species.append(sp)
         return sp
 
     # -- drivers (module-level routines) -----------------------------------
     def field_gathering_plus_particle_pusher(self):
         """particle_pusher_manager_3d.F90:50-112 with one tile spanning the
-        domain: zero the particle fields, fused gather + push."""
+        domain: zero the particle fields, fused gather + push.  Tiled engine:
+        the fused gather + push + periodic wrap + Esirkepov deposition."""
+        if self._tiled is not None:
+            self._tiled.particle_step()
+            return
         fn = {1: field_gathering_plus_particle_pusher_1_1_1,
               2: field_gathering_plus_particle_pusher_2_2_2,
               3: field_gathering_plus_particle_pusher_3_3_3}[self.nox]
@@ -200,7 +261,10 @@ class PicsarModule:
                clight=self.clight)
 
     def particle_bcs(self):
-        """Periodic wrap of every species (particle_boundaries.F90:1109-1300)."""
+        """Periodic wrap of every species (particle_boundaries.F90:1109-1300).
+        Tiled engine: done by the fused particle kernel."""
+        if self._tiled is not None:
+            return
         for sp in self.species:
             if sp.np == 0:
                 continue
@@ -208,9 +272,41 @@ class PicsarModule:
                       _ptr(sp.part_z), self.xmin, self.ymin, self.zmin, self.xmax, self.ymax,
                       self.zmax, _stream())
 
+    def pxr_particle_sorting(self):
+        """sorting.F90:67-215: when sorting_activated, every species whose
+        sorting_period divides `it` (from sorting_start on) is sorted by
+        cell bin (bins sorting_dx x sorting_dy x sorting_dz from the domain
+        start plus the shifts; one tile spanning the domain).  Tiled engine:
+        the engine's own counting sort by cell tile and bank order."""
+        if self.sorting_activated <= 0:
+            return
+        for sp in self.species:
+            if not (self.it >= sp.sorting_start and sp.sorting_period > 0
+                    and self.it % sp.sorting_period == 0) or sp.np == 0:
+                continue
+            if self._tiled is not None:
+                self._tiled.sort()
+                continue
+            # one tile per axis takes both the first- and the last-tile branch of
+            # the reference's tile split (tiling.F90:154-185): its particle
+            # region, where the bins start, is [min - d/2, max)
+            lo = (self.xmin - self.dx / 2 + self.sorting_shiftx,
+                  self.ymin - self.dy / 2 + self.sorting_shifty,
+                  self.zmin - self.dz / 2 + self.sorting_shiftz)
+            hi = (self.xmax + self.sorting_dx, self.ymax + self.sorting_dy,
+                  self.zmax + self.sorting_dz)
+            pxr_particle_bin_sorting(sp.np, sp.part_x, sp.part_y, sp.part_z, sp.part_ux,
+                                     sp.part_uy, sp.part_uz, sp.part_gaminv, sp.pid_w,
+                                     *lo, *hi, self.sorting_dx, self.sorting_dy,
+                                     self.sorting_dz, module=self)
+
     def pxrdepose_currents_on_grid_jxjyjz(self):
         """J = 0, then Esirkepov deposition of every species
-        (current_deposition_manager_3d.F90:224-494, currdepo = 0)."""
+        (current_deposition_manager_3d.F90:224-494, currdepo = 0).  Tiled
+        engine: J was deposited by the fused particle kernel."""
+        if self._tiled is not None:
+            self._tiled.check_deposited()
+            return
         self.jx.zero_(); self.jy.zero_(); self.jz.zero_()
         for sp in self.species:
             if sp.np == 0 or not sp.ldodepos:
@@ -223,13 +319,20 @@ class PicsarModule:
                           self.currdepo, err_flag=self._err)
 
     def current_bcs(self):
+        if self._tiled is not None:
+            return                  # the engine deposits J with periodic wrapping
         _summation_bcs(self.jx, self.jy, self.jz, self.nx, self.ny, self.nz, self.nxjguards)
 
     def charge_bcs(self):
+        if self._tiled is not None:
+            return
         _summation_bcs(self.rho, None, None, self.nx, self.ny, self.nz, self.nxjguards)
 
     def push_bfield(self):
         """B half step, order-2 Yee (maxwell_solver_manager.F90:44-85)."""
+        if self._tiled is not None:
+            self._tiled.push_b()
+            return
         n = (self.nx, self.ny, self.nz)
         g = self.nxguards
         pxrpush_em3d_bvec((0, 0, 0), n, (0, 0, 0), n, (0, 0, 0), n,
@@ -244,6 +347,9 @@ class PicsarModule:
 
     def push_efield(self):
         """E full step (maxwell_solver_manager.F90:393-439)."""
+        if self._tiled is not None:
+            self._tiled.push_e()
+            return
         n = (self.nx, self.ny, self.nz)
         g = self.nxguards
         lo, hi = (-g,) * 3, tuple(v + g for v in n)
@@ -256,12 +362,19 @@ class PicsarModule:
                           c2 * self.dt / self.dy, c2 * self.dt / self.dz)
 
     def efield_bcs(self):
+        if self._tiled is not None:
+            return                  # guards written by the engine's Yee kernels
         _field_bc(self.ex, self.ey, self.ez, self.nx, self.ny, self.nz, self.nxguards)
 
     def bfield_bcs(self):
+        if self._tiled is not None:
+            return
         _field_bc(self.bx, self.by, self.bz, self.nx, self.ny, self.nz, self.nxguards)
 
     def pxrdepose_rho_on_grid(self):
+        if self._tiled is not None:
+            self._tiled.deposit_rho()
+            return
         self.rho.zero_()
         for sp in self.species:
             if sp.np == 0:
@@ -278,10 +391,22 @@ class PicsarModule:
         self.charge_bcs()
 
     def step(self, nst=1, diags=False):
-        """PIC loop of src/submain.F90:104-195 (Yee solver, l_plasma)."""
+        """PIC loop of src/submain.F90:104-195 (Yee solver, l_plasma).  Tiled
+        engine: one fused particle kernel and three Yee launches per step,
+        with the engine's own sort and re-layout schedule."""
+        if self._tiled is not None:
+            for _ in range(nst):
+                self._tiled.step()
+                if self.sorting_activated > 0:
+                    self.pxr_particle_sorting()
+                if diags:
+                    self.calc_diags()
+                self.it += 1
+            return
         for _ in range(nst):
             self.field_gathering_plus_particle_pusher()
             self.particle_bcs()
+            self.pxr_particle_sorting()
             self.pxrdepose_currents_on_grid_jxjyjz()
             self.current_bcs()
             self.push_bfield(); self.bfield_bcs()
@@ -292,8 +417,240 @@ class PicsarModule:
             self.it += 1
 
     def check_errors(self):
+        if self._tiled is not None:
+            self._tiled.check_errors()
         if int(self._err.item()) != 0:
             raise PicsarB200Error("a particle moved more than one cell in one step")
+
+    def diagnostics(self, gauss=True):
+        """FP64 energies (kinetic, E, B) and the Gauss-law residual of the
+        current state (diags.F90:847-1358); tiled engine only."""
+        if self._tiled is None:
+            raise PicsarB200Error("diagnostics() reads the tiled engine's FP64 sums")
+        self._tiled.flush()
+        return self._tiled.sim.diagnostics(gauss=gauss)
+
+
+for _name in _GRIDS:
+    setattr(PicsarModule, _name, _grid_property(_name))
+del _name
+
+
+class _TiledSpecies:
+    """A species of a tiled-engine PicsarModule: ``part_x`` ... ``part_gaminv``,
+    ``pid_w`` (weight) and ``pid_id`` read as PICSAR FP64 arrays in the
+    order the particles were added (the engine sorts internally and tracks
+    ids).  Arrays that were read are written back into the engine before its
+    next operation, so they may be edited in place; the engine recomputes
+    gamma from u, so edits of ``part_gaminv`` alone have no effect."""
+
+    _COLS = {"part_x": "x", "part_y": "y", "part_z": "z", "part_ux": "ux", "part_uy": "uy",
+             "part_uz": "uz", "part_gaminv": "gaminv", "pid_w": "w", "pid_id": "id"}
+
+    def __init__(self, state, name, charge, mass):
+        self._state = state
+        self.name, self.charge, self.mass = name, float(charge), float(mass)
+        self.ldodepos = True
+        self.sorting_period = self.sorting_start = 0
+
+    @property
+    def np(self):
+        return self._state.sim.np
+
+    def __getattr__(self, attr):
+        if attr in _TiledSpecies._COLS:
+            return self._state.particle_views()[_TiledSpecies._COLS[attr]]
+        if attr in ("part_ex", "part_ey", "part_ez", "part_bx", "part_by", "part_bz"):
+            raise AttributeError(
+                f"{attr}: the tiled engine gathers E and B inside its fused particle kernel "
+                "and keeps no per-particle field arrays (use engine='plain')")
+        raise AttributeError(attr)
+
+
+class _TiledState:
+    """The tiled engine behind a PicsarModule: the simulation in the engine's
+    layout, plus PICSAR-layout views of the module arrays and particles.
+
+    A view is valid while the engine has not changed what it shows; reading
+    a module array exports it if needed.  Views handed out (read or set)
+    since the last engine operation are imported back before the next one."""
+
+    _WHICH = {"ex": 0, "ey": 1, "ez": 2, "bx": 3, "by": 4, "bz": 5, "jx": 6, "jy": 7, "jz": 8}
+
+    def __init__(self, m, precision, config):
+        from .tiled import TiledConfig, TiledSim
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        if not (m.nxguards == m.nyguards == m.nzguards):
+            raise ValueError("the tiled engine takes equal guard counts on all axes")
+        self.m = m
+        cfg = config or TiledConfig(tile=(8, 8, 8))
+        self.sim = TiledSim((m.nx, m.ny, m.nz), order=m.nox, pusher=m.particle_pusher,
+                            precision=precision, d=(m.dx, m.dy, m.dz),
+                            xmin=(m.xmin, m.ymin, m.zmin), dt=m.dt, clight=m.clight,
+                            mu0=m.mu0, eps0=m.eps0, config=cfg, track_ids=True,
+                            device=m.device)
+        self.ng = m.nxguards
+        self.views, self.valid, self.out = {}, set(), set()
+        self.pviews, self.pvalid, self.pout = None, False, False
+        self.species = None
+        self.deposited = False
+
+    # -- module arrays --------------------------------------------------------
+    def _view(self, name):
+        v = self.views.get(name)
+        if v is None:
+            m = self.m
+            v = grid_zeros(m.nx, m.ny, m.nz, self.ng, device=m.device)
+            self.views[name] = v
+        return v
+
+    def grid(self, name):
+        v = self._view(name)
+        if name not in self.valid:
+            if name in self._WHICH:
+                _lib.call("pxrb_tiled_field_export", self.sim._jp(), self._WHICH[name],
+                          v.data_ptr(), self.ng, _stream())
+            elif name == "rho":
+                self._export_rho(v)
+            self.valid.add(name)
+        self.out.add(name)
+        return v
+
+    def set_grid(self, name, value):
+        v = self._view(name)
+        if value is not v:
+            v.copy_(torch.as_tensor(value).to(v.device, torch.float64))
+        self.valid.add(name)
+        self.out.add(name)
+
+    def _export_rho(self, v):
+        m, g = self.m, self.ng
+        idx = lambda n: torch.remainder(torch.arange(-g, n + g + 1, device=m.device), n)
+        r = self.sim.rho.view(m.nz, m.ny, m.nx)
+        v.copy_(r[idx(m.nz)][:, idx(m.ny)][:, :, idx(m.nx)].permute(2, 1, 0))
+
+    # -- particles ------------------------------------------------------------
+    def add_species(self, name, charge, mass, x, y, z, ux, uy, uz, w, pid):
+        if self.species is not None:
+            raise NotImplementedError("the tiled engine pushes one species per module; use "
+                                      "engine='plain' for several")
+        sim = self.sim
+        sim.q, sim.m = float(charge), float(mass)
+        sim._fill_job()
+        self.flush()
+        sim.load_particles(x, y, z, ux, uy, uz, w, ids=pid)
+        self.species = _TiledSpecies(self, name, charge, mass)
+        self.pvalid = False
+        return self.species
+
+    def particle_views(self):
+        if not self.pvalid:
+            p = self.sim.particles()
+            p["id"] = p["id"].to(torch.float64)
+            self.pviews = p
+            self.pvalid = True
+        self.pout = True
+        return self.pviews
+
+    # -- engine operations ----------------------------------------------------
+    def flush(self):
+        """Write handed-out views back and follow changed module variables."""
+        m, sim = self.m, self.sim
+        if m.nox != sim.order:
+            raise PicsarB200Error("nox changed after the tiled engine was built; build a new "
+                                  "PicsarModule for another shape order")
+        if m.particle_pusher != sim.pusher or m.dt != sim.dt:
+            sim._pull_job()
+            sim.pusher, sim.dt = int(m.particle_pusher), float(m.dt)
+            sim.job.pusher, sim.job.dt = sim.pusher, sim.dt
+            sim._push_job()
+        for name in sorted(self.out):
+            if name in self._WHICH:
+                _lib.call("pxrb_tiled_field_import", sim._jp(), self._WHICH[name],
+                          self.views[name].data_ptr(), self.ng, _stream())
+        self.out.clear()
+        if self.pout and self.pviews is not None:
+            p = self.pviews
+            sim.load_particles(p["x"], p["y"], p["z"], p["ux"], p["uy"], p["uz"], p["w"],
+                               ids=p["id"].to(torch.int32))
+            self.pvalid = False
+        self.pout = False
+
+    def particle_step(self):
+        self.flush()
+        sim = self.sim
+        if getattr(sim, "_j_dirty", False):
+            for t in sim.J:
+                t.zero_()
+            sim._j_dirty = False
+        sim.particle_step()
+        sim.it += 1
+        sim.housekeeping()
+        self.deposited = True
+        self.valid -= {"jx", "jy", "jz", "rho"}
+        self.pvalid = False
+
+    def check_deposited(self):
+        if not self.deposited:
+            raise PicsarB200Error("tiled engine: the current is deposited by the fused "
+                                  "particle kernel; call field_gathering_plus_particle_pusher "
+                                  "first")
+
+    def push_b(self):
+        self.flush()
+        self.sim.push_b(0.5)
+        self.valid -= {"bx", "by", "bz"}
+
+    def push_e(self):
+        self.flush()
+        self.sim.push_e(zero_j=False)
+        self.sim._j_dirty = True          # the next particle kernel starts from J = 0
+        self.deposited = False
+        self.valid -= {"ex", "ey", "ez"}
+
+    def step(self):
+        self.flush()
+        self.sim.step(1, keep_j=True)
+        self.deposited = False
+        self.valid.clear()
+        self.pvalid = False
+
+    def sort(self):
+        self.flush()
+        self.sim.sort()
+        self.pvalid = False
+
+    def deposit_rho(self):
+        self.flush()
+        self.sim.diagnostics(gauss=True, to_host=False)
+        self.valid.discard("rho")
+
+    def check_errors(self):
+        if self.sim.error_flag():
+            raise PicsarB200Error("a particle moved more than one cell in one step")
+
+
+def pxr_particle_bin_sorting(np2, xp, yp, zp, ux, uy, uz, gam, pid, xmin2, ymin2, zmin2,
+                             xmax2, ymax2, zmax2, dxf, dyf, dzf, wpid=1, module=None):
+    """sorting.F90:247: stable sort of the particle arrays by cell bin, in
+    place.  pid: the weight column (1-D), the only pid column the reference
+    carries along, or None.  Scratch comes from torch (kept on ``module``
+    when given)."""
+    n = int(np2)
+    if n == 0:
+        return
+    need = _lib.query("pxrb_particle_bin_sorting_scratch", n)
+    scr = getattr(module, "_sort_scratch", None) if module is not None else None
+    if scr is None or scr.numel() < need:
+        scr = torch.empty(need, dtype=torch.uint8, device=xp.device)
+        if module is not None:
+            module._sort_scratch = scr
+    _lib.call("pxrb_particle_bin_sorting", n,
+              *[_ptr(a) for a in (xp, yp, zp, ux, uy, uz, gam)],
+              None if pid is None else _ptr(pid, "pid"), float(xmin2), float(ymin2),
+              float(zmin2), float(xmax2), float(ymax2), float(zmax2), float(dxf), float(dyf),
+              float(dzf), scr.data_ptr(), scr.numel(), _stream())
 
 
 def _field_bc(a, b, c, nx, ny, nz, g):

@@ -338,10 +338,16 @@ class TiledSim:
                 self._j_dirty = True
             self.push_b(0.5)
             self.it += 1
-            if self.cfg.sort_interval > 0 and self.it % self.cfg.sort_interval == 0:
-                self.sort()
-            elif self.cfg.relayout_interval > 0 and self.it % self.cfg.relayout_interval == 0:
-                self.relayout()
+            self.housekeeping()
+
+    def housekeeping(self):
+        """The engine's particle-order schedule after step `it`: the sort every
+        sort_interval steps, the bank re-layout every relayout_interval steps
+        between sorts."""
+        if self.cfg.sort_interval > 0 and self.it % self.cfg.sort_interval == 0:
+            self.sort()
+        elif self.cfg.relayout_interval > 0 and self.it % self.cfg.relayout_interval == 0:
+            self.relayout()
 
     # ----------------------------------------------------------- diagnostics
     def diagnostics(self, gauss=True, to_host=True):

@@ -241,3 +241,25 @@ def test_golden_fixtures_reproduce():
         tag = make_golden.tag(**case)
         for k, v in out.items():
             np.testing.assert_array_equal(v, fx[f"{tag}/{k}"], err_msg=f"{tag}/{k}")
+
+
+def test_bin_sorting_is_a_stable_sort_by_bin():
+    """The oracle's pxr_particle_bin_sorting (sorting.F90:247-361) equals a
+    stable argsort by the reference's bin number."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(5)
+    n = 5000
+    lo, hi, d = (0.0, -1.0, 2.0), (8.0, 5.0, 12.0), (1.0, 0.5, 2.0)
+    x = rng.uniform(lo[0], hi[0], n)
+    y = rng.uniform(lo[1], hi[1], n)
+    z = rng.uniform(lo[2], hi[2], n)
+    cols = [x, y, z] + [rng.standard_normal(n) for _ in range(4)] + [np.arange(n, dtype=np.float64)]
+    nb = [int(np.ceil((h - l) / dd)) for l, h, dd in zip(lo, hi, d)]
+    key = (np.floor((z - lo[2]) / d[2]) * nb[0] * nb[1] + np.floor((y - lo[1]) / d[1]) * nb[0]
+           + np.floor((x - lo[0]) / d[0])).astype(np.int64)
+    perm = np.argsort(key, kind="stable")
+    want = [c[perm] for c in cols]
+    got = [c.copy() for c in cols]
+    O.particle_bin_sorting(*got, lo, hi, d)
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
