@@ -234,29 +234,58 @@ def cpu_oracle_rate(wl, steps, warmup, threads=None):
 
 
 def run_reference(args):
+    """Reference arm: the oracle (PICSAR's routines restated, OpenMP over
+    16^3-cell tiles, all host cores) on the full workload configuration --
+    the same grid, particle count, shape order and pusher as this
+    framework's line.  The metric is a rate, so each timed step is one full
+    PIC step of the whole state; the step counts are capped (warm-up 1,
+    timed 2) to keep the run within minutes."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     if args.workload in ("ensemble", "serve"):
         return run_reference_jobs(args)
+    from oracle import oracle as O
     wl = WORKLOADS[args.workload]
-    threads = os.cpu_count()
-    rate, el, np_, nth = cpu_oracle_rate(wl, args.steps, args.warmup, threads)
+    os.environ["OMP_NUM_THREADS"] = str(os.cpu_count())
+    n = wl["n"]
+    st = _initial_state(wl, 1234, device="cpu").numpy()
+    N = len(st["x"])
+    o = O.OracleSim(n, 3, order=wl["order"], pusher=wl["pusher"],
+                    tiles=tuple(max(1, v // 16) for v in n),
+                    sorting_period=wl["sort_interval"])
+    t0 = time.perf_counter()
+    o.add_particles(st["x"], st["y"], st["z"], st["ux"], st["uy"], st["uz"], st["w"])
+    t_load = time.perf_counter() - t0
+    del st
+    warm, steps = min(args.warmup, 1), max(1, min(args.steps, 2))
+    o.step(warm)
+    t0 = time.perf_counter()
+    o.step(steps)
+    el = time.perf_counter() - t0
+    rate = N * steps / el
+    nth = O.num_threads()
+    ncell = n[0] * n[1] * n[2]
     line = {
         "impl": "reference", "metric": "particle-steps/s", "value": rate,
-        "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "unit": "particle-steps/s", "n_gpus": ws, "steps": steps, "warmup": warm,
+        "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl["desc"], "sample": f"32^3 cells, {np_} particles per step"},
+        "config": {"workload": wl["desc"], "particles": N, "cells": ncell,
+                   "sample": f"the full workload: {steps} timed PIC steps after {warm} "
+                             f"warm-up (steps capped from --steps {args.steps} / --warmup "
+                             f"{args.warmup}; the metric is a rate)"},
         "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": nth,
                          "kind": "port",
-                         "sample": f"{args.steps} PIC steps of a 32^3-cell, {np_}-particle "
-                                   f"sample of the workload, tiles 4^3, OpenMP"},
+                         "sample": f"{steps} PIC steps of the full {N}-particle, {ncell}-cell "
+                                   f"workload, OpenMP over 16^3-cell tiles "
+                                   f"(load {t_load:.1f} s untimed)"},
         "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "note": "PICSAR's Fortran cannot be compiled in this image (no Fortran compiler); "
-                "the reference arm runs the line-by-line C++ restatement of its routines",
+                "the reference arm runs the line-by-line C++ restatement of its routines, "
+                "whose kernels are pinned bit for bit to the reference's own routines",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -382,28 +411,47 @@ def run_ours(args):
     # end-to-end through the public API with host buffers
     e2e = None
     if not args.skip_e2e:
-        e2e = run_e2e(sim, st, wl, args, ws)
+        del sim
+        torch.cuda.empty_cache()
+        e2e = run_e2e(st, wl, args, ws, cfg)
+    else:
+        del sim
     del st
-
-    del sim
     torch.cuda.empty_cache()
     # plain FP64 GPU path on the same workload (the comparison baseline)
     fp64 = None
     if not args.skip_fp64:
         fp64 = run_plain_fp64(wl, args, ws, rank)
 
-    # FP32 mixed vs FP64 on the same state: one-step error, energy and
-    # Gauss-law drift over the run, for each pusher
+    # the tiled engine in FP64 on the same workload (the same engine, 1e-12
+    # of the oracle), with its roofline
+    fp64_tiled = None
+    if not args.skip_fp64 and prec == 0:
+        fp64_tiled = run_tiled_fp64(wl, args, ws, rank, cfg)
+
+    # FP32 mixed vs FP64 vs the oracle from one developed state: one-step
+    # error, energy and Gauss-law drift and field spectra over the run, for
+    # each pusher (rank 0: the oracle runs on the host cores)
     accuracy = None
-    if not args.skip_accuracy and args.precision == "fp32":
-        accuracy = [run_accuracy(wl, args, p, cfg) for p in (0, 1)]
+    if rank == 0 and not args.skip_accuracy and args.precision == "fp32":
+        accuracy = [run_accuracy(wl, args, p, cfg, with_oracle=not args.skip_cpu)
+                    for p in (0, 1)]
 
     cpu = None
     if rank == 0 and not args.skip_cpu:
-        rate, el, np_, nth = cpu_oracle_rate(wl, args.cpu_steps, 1, os.cpu_count())
-        cpu = {"value": rate, "unit": "particle-steps/s", "cores": nth, "kind": "port",
-               "sample": f"{args.cpu_steps} PIC steps of a 32^3-cell, {np_}-particle sample "
-                         f"of the workload (oracle, OpenMP over 4^3 tiles), {el:.1f} s"}
+        orc = accuracy[0].get("oracle") if accuracy else None
+        if orc:
+            cpu = {"value": orc["particle_steps_per_s"], "unit": "particle-steps/s",
+                   "cores": orc["threads"], "kind": "port",
+                   "sample": f"1 PIC step of the full workload ({orc['particles']} particles, "
+                             f"{ncell} cells) from its developed state (oracle, OpenMP over "
+                             f"16^3-cell tiles), {orc['step_seconds']:.1f} s"}
+        else:
+            rate, el, np_, nth = cpu_oracle_rate(wl, args.cpu_steps, 1, os.cpu_count())
+            cpu = {"value": rate, "unit": "particle-steps/s", "cores": nth, "kind": "port",
+                   "sample": f"{args.cpu_steps} PIC steps of a 32^3-cell, {np_}-particle "
+                             f"sample of the workload (oracle, OpenMP over 4^3 tiles), "
+                             f"{el:.1f} s"}
     if rank == 0:
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
@@ -434,6 +482,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clk,
             "fp64_plain": fp64,
+            "fp64_tiled": fp64_tiled,
             "energy": {"start": e0["total"], "end": e1["total"],
                        "rel_change": (e1["total"] - e0["total"]) / e0["total"]},
             "slow_path_particle_steps": slow,
@@ -460,55 +509,207 @@ def _smem_roofline(wl, prec, cfg, N, kern_ms, clk):
             "rates_warp_inst_per_clk_sm": SMEM_RATE, "sm_mhz": mhz}
 
 
-def run_accuracy(wl, args, pusher, cfg):
-    """FP32 mixed against FP64 (the tiled FP64 engine, itself within 1e-12
-    of the oracle) from one identical state of the workload: relative L2
-    error of E, B and particle momenta after one step; total-energy drift
-    (from step 1, the first step with a kinetic energy sum) and Gauss-law
-    residual drift (from the loaded state) after `accuracy_steps` steps, in
-    both precisions."""
+DEV_STEPS = 10            # FP64 steps that develop the fields before the comparisons
+B0 = (0.0, 0.0, 0.5)      # uniform magnetic field of the accuracy legs (omega_c = omega_p / 2)
+SPECTRUM_SHELLS = (1, 2, 4, 8, 16, 32, 64, 128)
+
+
+def _developed_state(wl, pusher, cfg64):
+    """The workload's seeded plasma in a uniform field B0, stepped DEV_STEPS
+    times by the FP64 tiled engine: E and B grown from the particles' own
+    currents plus B0, so both pushers' rotation terms are exercised.
+    Returns the state as PICSAR FP64 arrays: fields (3 guards) and particles
+    in id order."""
     import torch
-    from picsar_b200.init import thermal_plasma
-    from picsar_b200.tiled import TiledConfig, TiledSim
+    from picsar_b200.picsar import grid_zeros
+    from picsar_b200.tiled import TiledSim
+    st = _initial_state(wl, 4321)
+    t = TiledSim(wl["n"], order=wl["order"], pusher=pusher, precision="fp64", config=cfg64,
+                 track_ids=True)
+    for name, v in zip(("bx", "by", "bz"), B0):
+        if v:
+            t.import_field(name, grid_zeros(*wl["n"], 3).fill_(v), 3)
+    t.load_state(st)
+    del st
+    t.step(DEV_STEPS)
+    f = {n: t.export_field(n, 3) for n in ("ex", "ey", "ez", "bx", "by", "bz")}
+    p = t.particles()
+    del t
+    torch.cuda.empty_cache()
+    return f, p
+
+
+def _sim_from_state(wl, prec, pusher, cfg, f, p):
+    from picsar_b200.tiled import TiledSim
+    t = TiledSim(wl["n"], order=wl["order"], pusher=pusher, precision=prec, config=cfg,
+                 track_ids=True)
+    for name, a in f.items():
+        t.import_field(name, a, 3)
+    t.load_particles(p["x"], p["y"], p["z"], p["ux"], p["uy"], p["uz"], p["w"], ids=p["id"])
+    return t
+
+
+def _field_spectrum(sim, names):
+    """Shell-averaged power sum_c |FFT(F_c)|^2 over the periodic nodes,
+    shells of integer |k| (k in grid wave numbers)."""
+    import torch
+    nx, ny, nz = sim.n
+    tot = None
+    for name in names:
+        a = sim.export_field(name, 3)[3:3 + nx, 3:3 + ny, 3:3 + nz]
+        F = torch.fft.fftn(a)
+        pw = F.real ** 2 + F.imag ** 2
+        del F
+        tot = pw if tot is None else tot + pw
+    dev = tot.device
+    k = [torch.fft.fftfreq(n, d=1.0 / n, device=dev, dtype=torch.float64) for n in (nx, ny, nz)]
+    kk = torch.sqrt(k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 +
+                    k[2][None, None, :] ** 2)
+    shell = torch.round(kk).long().flatten()
+    spec = torch.bincount(shell, weights=tot.flatten()) / torch.bincount(shell).clamp(min=1)
+    return spec.cpu().numpy()
+
+
+def _spectra_ratio(s32, s64, kmax):
+    import numpy as np
+    r = s32[1:kmax + 1] / np.maximum(s64[1:kmax + 1], 1e-300)
+    return {"ratio_fp32_over_fp64_median": float(np.median(r)),
+            "ratio_min": float(r.min()), "ratio_max": float(r.max()),
+            "shells": {str(k): {"fp64": float(s64[k]), "ratio": float(s32[k] / s64[k])}
+                       for k in SPECTRUM_SHELLS if k <= kmax}}
+
+
+def _rel_l2_t(a, b):
+    import torch
+    return float(torch.linalg.norm(a - b) / torch.linalg.norm(b).clamp(min=1e-300))
+
+
+def _oracle_one_step(wl, pusher, f, p):
+    """The oracle (all host cores, OpenMP over 16^3-cell tiles) one step from
+    the exported state.  Returns its fields E, B, J (GPU tensors, PICSAR
+    layout), particle columns in id order (GPU) and the step's seconds."""
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+    n = wl["n"]
+    os.environ["OMP_NUM_THREADS"] = str(os.cpu_count())
+    o = O.OracleSim(n, 3, order=wl["order"], pusher=pusher,
+                    tiles=tuple(max(1, v // 16) for v in n))
+    for name, a in f.items():
+        o.set_field(name, a.cpu().numpy())
+    host = {c: p[c].cpu().numpy() for c in ("x", "y", "z", "ux", "uy", "uz", "w")}
+    ids = p["id"].to(torch.float64).cpu().numpy()
+    t0 = time.perf_counter()
+    o.add_particles(host["x"], host["y"], host["z"], host["ux"], host["uy"], host["uz"],
+                    host["w"], pid=ids)
+    t_load = time.perf_counter() - t0
+    del host, ids
+    t0 = time.perf_counter()
+    o.step(1)
+    el = time.perf_counter() - t0
+    fields = {}
+    for name in ("ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz"):
+        a = np.asfortranarray(o.get_field(name))
+        fields[name] = torch.from_numpy(a).cuda()
+    cols = o.columns(["x", "y", "z", "ux", "uy", "uz", "id"])
+    nth = O.num_threads()
+    del o
+    idx = torch.from_numpy(cols.pop("id").astype(np.int64)).cuda()
+    parts = {}
+    for c, v in cols.items():
+        t = torch.empty(len(v), dtype=torch.float64, device="cuda")
+        t[idx] = torch.from_numpy(v).cuda()
+        parts[c] = t
+    return fields, parts, el, t_load, nth
+
+
+def run_accuracy(wl, args, pusher, cfg, with_oracle=True):
+    """FP32 mixed against FP64 and both against the oracle, from a developed
+    state of the full workload (uniform B0 plus DEV_STEPS FP64 steps; the
+    same exported PICSAR-layout state loaded into each):
+      * one step: relative L2 of E, B, J and of the particle momenta and
+        positions, FP32 tiled and FP64 tiled against the oracle (the
+        reference's routines restated, all host cores) and FP32 against FP64;
+      * `accuracy_steps` steps: total-energy drift (from step 1, the first
+        step with a kinetic energy sum), Gauss-law residual drift, and the
+        shell-averaged E and B power spectra at steps 0, steps/2 and steps."""
+    import torch
+    from picsar_b200.tiled import SUPPORTED_SHAPES_FP64, TiledConfig
+    t0 = time.perf_counter()
     cfg = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval, drift=cfg.drift,
                       threads=cfg.threads, acc=cfg.acc, relayout_interval=cfg.relayout_interval)
-    st = _initial_state(wl, 4321)
-    steps = args.accuracy_steps
-    sims, one = {}, {}
-    t0 = time.perf_counter()
-    from picsar_b200.tiled import SUPPORTED_SHAPES_FP64
     cfg64 = cfg
     if (cfg.tile[0], cfg.drift) not in SUPPORTED_SHAPES_FP64:
         cfg64 = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval,
                             drift=min(cfg.drift, 1), threads=cfg.threads,
                             relayout_interval=cfg.relayout_interval)
-    for prec in ("fp64", "fp32"):
-        t = TiledSim(wl["n"], order=wl["order"], pusher=pusher, precision=prec,
-                     config=cfg64 if prec == "fp64" else cfg, track_ids=True)
-        t.load_state(st)
-        g0 = t.diagnostics(gauss=True)["gauss_norm"]
-        t.step(1)
-        d1 = t.diagnostics(gauss=False)
-        f = {n: t.export_field(n, 3) for n in ("ex", "ey", "ez", "bx", "by", "bz")}
+    f, p = _developed_state(wl, pusher, cfg64)
+    steps = args.accuracy_steps
+    sims = {"fp64": _sim_from_state(wl, "fp64", pusher, cfg64, f, p),
+            "fp32": _sim_from_state(wl, "fp32", pusher, cfg, f, p)}
+    kmax = min(wl["n"]) // 2
+    spectra = {"E": {}, "B": {}}
+    spec0 = {prec: {"E": _field_spectrum(t, ("ex", "ey", "ez")),
+                    "B": _field_spectrum(t, ("bx", "by", "bz"))} for prec, t in sims.items()}
+    for fl in ("E", "B"):
+        spectra[fl]["0"] = _spectra_ratio(spec0["fp32"][fl], spec0["fp64"][fl], kmax)
+    g0, d1, one = {}, {}, {}
+    for prec, t in sims.items():
+        g0[prec] = t.diagnostics(gauss=True)["gauss_norm"]
+        t.step(1, keep_j=True)
+        d1[prec] = t.diagnostics(gauss=False)
+        fl = {n: t.export_field(n, 3) for n in ("ex", "ey", "ez", "bx", "by", "bz",
+                                                   "jx", "jy", "jz")}
         pp = t.particles()
-        f.update({c: pp[c] for c in ("ux", "uy", "uz")})
+        fl.update({c: pp[c] for c in ("x", "y", "z", "ux", "uy", "uz")})
         del pp
-        one[prec] = f
-        sims[prec] = (t, g0, d1)
-    del st
-    err = {k: float(torch.linalg.norm(one["fp32"][k] - one["fp64"][k]) /
-                    torch.linalg.norm(one["fp64"][k])) for k in one["fp64"]}
-    del one
-    torch.cuda.empty_cache()
+        one[prec] = fl
     res = {"pusher": "Vay" if pusher else "Boris", "steps": steps,
-           "one_step_rel_l2_fp32_vs_fp64": err}
-    for prec, (t, g0, d1) in sims.items():
-        t.step(steps - 1)
+           "state": f"seeded plasma in a uniform B = {list(B0)}, then {DEV_STEPS} FP64 steps",
+           "one_step_rel_l2": {}}
+
+    def errs(a, b):
+        out = {}
+        for k in b:
+            if k in ("x", "y", "z"):
+                L = float(wl["n"]["xyz".index(k)])
+                d = torch.remainder(a[k] - b[k] + L / 2, L) - L / 2
+                out[k] = float(torch.linalg.norm(d) / torch.linalg.norm(b[k]))
+            else:
+                out[k] = _rel_l2_t(a[k], b[k])
+        return out
+    res["one_step_rel_l2"]["fp32_vs_fp64"] = errs(one["fp32"], one["fp64"])
+    if with_oracle:
+        of, op, el, t_load, nth = _oracle_one_step(wl, pusher, f, p)
+        ref = dict(of)
+        ref.update(op)
+        res["one_step_rel_l2"]["fp64_vs_oracle"] = errs(one["fp64"], ref)
+        res["one_step_rel_l2"]["fp32_vs_oracle"] = errs(one["fp32"], ref)
+        res["oracle"] = {"step_seconds": el, "load_seconds": t_load, "threads": nth,
+                         "particles": int(p["x"].numel()),
+                         "particle_steps_per_s": p["x"].numel() / el}
+        del of, op, ref
+    del one, f, p
+    torch.cuda.empty_cache()
+    half = max(1, steps // 2)
+    for prec, t in sims.items():
+        t.step(half - 1)
+        spec0[prec]["E_half"] = _field_spectrum(t, ("ex", "ey", "ez"))
+        spec0[prec]["B_half"] = _field_spectrum(t, ("bx", "by", "bz"))
+        t.step(steps - half)
         d = t.diagnostics(gauss=True)
-        res[prec] = {"energy_drift": (d["total"] - d1["total"]) / d1["total"],
-                     "gauss_residual_start": g0, "gauss_residual_end": d["gauss_norm"],
-                     "gauss_residual_drift": abs(d["gauss_norm"] - g0) / g0,
+        spec0[prec]["E_end"] = _field_spectrum(t, ("ex", "ey", "ez"))
+        spec0[prec]["B_end"] = _field_spectrum(t, ("bx", "by", "bz"))
+        res[prec] = {"energy_drift": (d["total"] - d1[prec]["total"]) / d1[prec]["total"],
+                     "gauss_residual_start": g0[prec], "gauss_residual_end": d["gauss_norm"],
+                     "gauss_residual_drift": abs(d["gauss_norm"] - g0[prec]) / g0[prec],
                      "error_flag": t.error_flag()}
+    for fl in ("E", "B"):
+        spectra[fl][str(half)] = _spectra_ratio(spec0["fp32"][fl + "_half"],
+                                                spec0["fp64"][fl + "_half"], kmax)
+        spectra[fl][str(steps)] = _spectra_ratio(spec0["fp32"][fl + "_end"],
+                                                 spec0["fp64"][fl + "_end"], kmax)
+    res["field_spectra"] = spectra
     e32, e64 = abs(res["fp32"]["energy_drift"]), abs(res["fp64"]["energy_drift"])
     g32, g64 = res["fp32"]["gauss_residual_drift"], res["fp64"]["gauss_residual_drift"]
     res["energy_drift_ratio_fp32_over_fp64"] = e32 / e64 if e64 else None
@@ -521,44 +722,50 @@ def run_accuracy(wl, args, pusher, cfg):
     return res
 
 
-def run_e2e(sim, st, wl, args, ws):
-    """Same job through the public API from pinned host buffers: upload the
-    PICSAR particle arrays, run the steps reading the energies back every
-    step, download the final particle arrays."""
+def run_e2e(st, wl, args, ws, cfg):
+    """The same job end to end through the reference-facing module surface
+    (picsar_b200.picsar.PicsarModule on the tiled engine): the PICSAR FP64
+    particle arrays handed over from pinned host memory (add_species: upload,
+    conversion, sort), the steps with the FP64 energies copied back to the
+    host every step, and the particle arrays the steps change (x, y, z, u,
+    gamma^-1, in the order they were added) copied back at the end.  The
+    module is built before the timed region (field allocation)."""
     import torch
+    from picsar_b200.picsar import PicsarModule
     N = st.np
     host = {c: getattr(st, c).to("cpu").pin_memory() for c in ("x", "y", "z", "ux", "uy", "uz", "w")}
-    dev = {c: torch.empty(N, dtype=torch.float64, device="cuda") for c in host}
-    out_host = {c: torch.empty(N, dtype=torch.float64).pin_memory()
-                for c in ("x", "y", "z", "ux", "uy", "uz", "gaminv", "w")}
+    out_cols = ("part_x", "part_y", "part_z", "part_ux", "part_uy", "part_uz", "part_gaminv")
+    out_host = {c: torch.empty(N, dtype=torch.float64).pin_memory() for c in out_cols}
     diag_host = torch.empty((args.steps, 9), dtype=torch.float64).pin_memory()
+    m = PicsarModule(*wl["n"], nguards=3, nox=wl["order"], particle_pusher=wl["pusher"],
+                     engine="tiled", precision=args.precision, tiled_config=cfg)
     stream = torch.cuda.current_stream()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     _barrier(ws)
     w0 = time.perf_counter()
     a.record(stream)
-    for c in host:
-        dev[c].copy_(host[c], non_blocking=True)
-    sim.load_particles(dev["x"], dev["y"], dev["z"], dev["ux"], dev["uy"], dev["uz"], dev["w"])
-    for s in range(args.steps):
-        sim.step(1)
-        d = sim.diagnostics(gauss=False, to_host=False)
-        diag_host[s].copy_(d, non_blocking=True)
-    out = sim.particles()
-    for c in out_host:
-        out_host[c].copy_(out[c], non_blocking=True)
+    m.add_species("electron", -1.0, 1.0, host["x"], host["y"], host["z"], host["ux"],
+                  host["uy"], host["uz"], host["w"])
+    for s_ in range(args.steps):
+        m.step(1)
+        diag_host[s_].copy_(m.diagnostics(gauss=False, to_host=False), non_blocking=True)
+    sp = m.species[0]
+    for c in out_cols:
+        out_host[c].copy_(getattr(sp, c), non_blocking=True)
     b.record(stream)
     _barrier(ws)
     wall = time.perf_counter() - w0
     ms = _max_over_ranks(a.elapsed_time(b), ws)
+    del m
+    torch.cuda.empty_cache()
     h2d = 7 * 8 * N
-    d2h = 8 * 8 * N + args.steps * 9 * 8
+    d2h = len(out_cols) * 8 * N + args.steps * 9 * 8
     return {"value": N * ws * args.steps / (ms * 1e-3), "unit": "particle-steps/s",
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
             "ms": ms, "wall_s": wall,
-            "what": "job: PICSAR arrays uploaded from pinned host memory, converted and "
-                    "sorted, all steps with the energies read back every step, final "
-                    "particle arrays downloaded"}
+            "what": "job through PicsarModule(engine='tiled'): PICSAR FP64 particle arrays "
+                    "from pinned host memory (add_species), every step with its FP64 energies "
+                    "copied to the host, final x, y, z, u, gamma^-1 arrays copied to the host"}
 
 
 def run_plain_fp64(wl, args, ws, rank):
@@ -586,6 +793,49 @@ def run_plain_fp64(wl, args, ws, rank):
             "steps": args.fp64_steps, "ms_per_step": ms / args.fp64_steps,
             "what": "plain FP64 GPU path: PICSAR guarded FP64 arrays, one thread per "
                     "particle, global FP64 atomics, separate bc kernels"}
+
+
+def run_tiled_fp64(wl, args, ws, rank, cfg):
+    """The tiled engine in FP64 on the workload: steps and particle-kernel
+    time (CUDA events), with the kernel's HBM roofline (FP64 layout: 60 B
+    read + 52 B written per particle, 96 B per cell)."""
+    import torch
+    from picsar_b200.tiled import SUPPORTED_SHAPES_FP64, TiledConfig, TiledSim
+    c64 = TiledConfig(tile=cfg.tile, drift=min(cfg.drift, 1), threads=cfg.threads,
+                      sort_interval=cfg.sort_interval, relayout_interval=0)
+    if (c64.tile[0], c64.drift) not in SUPPORTED_SHAPES_FP64:
+        return None
+    st = _initial_state(wl, 1234 + rank)
+    N = st.np
+    t = TiledSim(wl["n"], order=wl["order"], pusher=wl["pusher"], precision="fp64", config=c64)
+    t.load_state(st)
+    del st
+    t.step(2)
+    steps = max(args.fp64_steps, 4)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(ws)
+    a.record(stream)
+    for s_ in range(steps):
+        t.step(1, events=ev[s_])
+    b.record(stream)
+    _barrier(ws)
+    ms = _max_over_ranks(a.elapsed_time(b), ws)
+    kern = sum(x.elapsed_time(y) for x, y in ev) / steps
+    del t
+    torch.cuda.empty_cache()
+    peak, peak_kind = _peaks()
+    ncell = wl["n"][0] * wl["n"][1] * wl["n"][2]
+    alg = BYTES_PER_PARTICLE[1] * N + GRID_BYTES_PER_CELL[1] * ncell
+    return {"value": N * ws * steps / (ms * 1e-3), "unit": "particle-steps/s", "steps": steps,
+            "ms_per_step": ms / steps, "kernel_ms": kern,
+            "roofline": {"bound": "hbm", "achieved": alg / (kern * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": alg / (kern * 1e-3) / 1e9 / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg},
+            "what": "tiled engine in FP64 (within 1e-12 of the oracle), same tiles and sort "
+                    "interval, no re-layout (the FP64 kernel makes one pass)"}
 
 
 def _plain_fp64_jobs(specs, steps=2):
@@ -752,6 +1002,7 @@ def run_ensemble(args):
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
             "fp64_plain": fp64,
+            "fp64_tiled": fp64_tiled,
             "speedup_vs_fp64_plain": value / fp64["value"] if fp64 else None,
             "energy_drift": {"median_abs": float(statistics.median(abs(x) for x in drift)),
                              "max_abs": float(max(abs(x) for x in drift))},

@@ -99,6 +99,7 @@ def _declare(L):
     L.orc_sim_phase.argtypes = [vp, i64]
     L.orc_num_threads.restype = C.c_int
     L.orc_particle_bin_sorting.argtypes = [i64] + [P] * 8 + [f64] * 9
+    L.orc_sim_get_particle_columns.argtypes = [vp, P, i64, P]
 
 
 def _c(a):
@@ -276,6 +277,15 @@ class OracleSim:
             o = np.argsort(cols["id"], kind="stable")
             cols = {c: v[o] for c, v in cols.items()}
         return cols
+
+    def columns(self, names):
+        """Selected particle columns (PART_COLS names) in the oracle's tile
+        order, without copying the others (large particle counts)."""
+        np_ = lib().orc_sim_np(self.h)
+        idx = np.array([PART_COLS.index(c) for c in names], dtype=np.int64)
+        buf = np.empty(len(names) * np_, dtype=np.float64)
+        lib().orc_sim_get_particle_columns(self.h, _p(idx), len(names), _p(buf))
+        return {c: buf[i * np_:(i + 1) * np_] for i, c in enumerate(names)}
 
     def step(self, nsteps=1, diag=False):
         lib().orc_sim_step(self.h, nsteps, int(bool(diag)))

@@ -1619,6 +1619,24 @@ void orc_sim_get_particles(void* h, double* out) {
   }
 }
 
+// Copies selected particle columns out in tile order: cols[i] indexes the
+// column list of orc_sim_get_particles; out[i*np + k].
+void orc_sim_get_particle_columns(void* h, const i64* cols, i64 ncols, double* out) {
+  OSim* s = (OSim*)h;
+  const i64 np = orc_sim_np(h);
+  for (i64 c = 0; c < ncols; ++c) {
+    i64 k = 0;
+    for (auto& t : s->tiles) {
+      const std::vector<double>* all[] = {&t.x, &t.y, &t.z, &t.ux, &t.uy, &t.uz, &t.gi,
+                                          &t.ex, &t.ey, &t.ez, &t.bx, &t.by, &t.bz, &t.w,
+                                          &t.id};
+      const std::vector<double>& v = *all[cols[c]];
+      std::copy(v.begin(), v.end(), out + c * np + k);
+      k += t.np();
+    }
+  }
+}
+
 // Runs nsteps PIC steps.  diag != 0: deposit rho and compute div E after each step.
 void orc_sim_step(void* h, i64 nsteps, i64 diag) {
   OSim* s = (OSim*)h;

@@ -678,7 +678,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
     // Bound of one particle's contribution to one node of J_c:
     //   |q| w_max / (dt dV / d_c) * (max displacement along c in cells),
     // with the displacement bounded from max |u| of the tile's particles
-    // before the push plus the push's change |q| dt / m (|E| + c |B|).
+    // before the push and the largest change the push can make to |u| in
+    // the window's fields (below).
     // A node of the window receives deposits only from particles whose old
     // cell lies within L+H+3 cells of it along every axis, so the node sum
     // is bounded by (max particles per window cell) * (L+H+3)^3 contributions.
@@ -748,8 +749,18 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
         U2 = fmaxf(U2, s_max[2][w]); Wm = fmaxf(Wm, s_max[3][w]); Cm = fmaxf(Cm, s_max[4][w]);
       }
       const double c = sj.clight;
-      const double ub = sqrt((double)U2) +
-                        fabs(sj.q) / sj.m * sj.dt * (1.7320508075688772 * ((double)E + c * B));
+      // |u| after the push, from |u| before it (U2) and the window maxima of
+      // |E| and |B| (componentwise maxima, times sqrt 3).  With qdm = |q| dt / m
+      // and tau = qdm |B| / 2 (the rotation parameter of both pushers): Boris
+      // changes |u| only by its two half E kicks, |u'| <= |u| + qdm |E|; Vay
+      // gives |u + qdm E + (u x tau) / gamma| <= |u| (1 + tau) + qdm |E| before
+      // its rotation and scales that by at most (1 + t + t^2) / (1 + t^2) <=
+      // 1 + tau.  So |u'| <= (|u| (1 + tau) + qdm |E|) (1 + tau) bounds both; the
+      // last factor covers the FP32 rounding of the pushers.
+      const double qdm = fabs(sj.q) / sj.m * sj.dt;
+      const double tau = 0.5 * qdm * 1.7320508075688772 * (double)B;
+      const double ub = (sqrt((double)U2) * (1.0 + tau) + qdm * 1.7320508075688772 * (double)E) *
+                        (1.0 + tau) * 1.0001;
       const double vb = ub / sqrt(1.0 + ub * ub / (c * c));
       const double dV = sj.dx * sj.dy * sj.dz;
       constexpr int reach = L + H + 3;

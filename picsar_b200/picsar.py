@@ -422,13 +422,14 @@ class PicsarModule:
         if int(self._err.item()) != 0:
             raise PicsarB200Error("a particle moved more than one cell in one step")
 
-    def diagnostics(self, gauss=True):
+    def diagnostics(self, gauss=True, to_host=True):
         """FP64 energies (kinetic, E, B) and the Gauss-law residual of the
-        current state (diags.F90:847-1358); tiled engine only."""
+        current state (diags.F90:847-1358); tiled engine only.  to_host=False
+        leaves the 9 sums on the device (see TiledSim.diagnostics)."""
         if self._tiled is None:
             raise PicsarB200Error("diagnostics() reads the tiled engine's FP64 sums")
         self._tiled.flush()
-        return self._tiled.sim.diagnostics(gauss=gauss)
+        return self._tiled.sim.diagnostics(gauss=gauss, to_host=to_host)
 
 
 for _name in _GRIDS:
@@ -573,7 +574,8 @@ class _TiledState:
         if self.pout and self.pviews is not None:
             p = self.pviews
             sim.load_particles(p["x"], p["y"], p["z"], p["ux"], p["uy"], p["uz"], p["w"],
-                               ids=p["id"].to(torch.int32))
+                               ids=p["id"].to(torch.int32),
+                               ids_dense=getattr(sim, "_ids_dense", False))
             self.pvalid = False
         self.pout = False
 

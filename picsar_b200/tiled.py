@@ -213,10 +213,18 @@ class TiledSim:
         raw = self.job_dev.cpu().numpy().tobytes()
         C.memmove(C.addressof(self.job), raw, len(raw))
 
-    def load_particles(self, x, y, z, ux, uy, uz, w, ids=None):
-        """Load particles given as PICSAR arrays (absolute FP64 positions)."""
+    def load_particles(self, x, y, z, ux, uy, uz, w, ids=None, ids_dense=None):
+        """Load particles given as PICSAR arrays (absolute FP64 positions),
+        device tensors or host arrays (pinned host tensors are uploaded
+        without blocking the host).  ids (tracked ids only): the particles'
+        identifiers, by default 0..N-1; ids_dense: True when ids is a
+        permutation of 0..N-1 (then particles() restores the id order by a
+        scatter instead of a sort)."""
         dev = self.device
-        f64 = lambda a: torch.as_tensor(a, dtype=torch.float64).to(dev).contiguous()
+
+        def f64(a):
+            t = torch.as_tensor(a, dtype=torch.float64)
+            return t.to(dev, non_blocking=t.is_pinned()).contiguous()
         x, y, z, ux, uy, uz, w = (f64(a) for a in (x, y, z, ux, uy, uz, w))
         N = int(x.numel())
         if N > _I32MAX:
@@ -241,6 +249,7 @@ class TiledSim:
         if self.track_ids:
             idt = (torch.arange(N, dtype=torch.int32, device=dev) if ids is None
                    else torch.as_tensor(ids).to(dev, torch.int32))
+            self._ids_dense = ids is None or bool(ids_dense)
             self.pid, self.pid_b = idt.contiguous(), torch.empty(N, dtype=torch.int32, device=dev)
             j.pid, j.pid_b = self.pid.data_ptr(), self.pid_b.data_ptr()
         else:
@@ -405,13 +414,20 @@ class TiledSim:
                   *[out[c].data_ptr() for c in ("x", "y", "z", "ux", "uy", "uz", "gaminv", "w")],
                   _stream())
         if self.track_ids and self.job.pid:
-            pid = torch.empty(N, dtype=torch.int32, device=dev)
             C_ptr = self.job.pid
             cur = self.pid if self.pid.data_ptr() == C_ptr else self.pid_b
-            pid.copy_(cur)
-            order = torch.argsort(pid.long())
-            out = {k: v[order] for k, v in out.items()}
-            out["id"] = pid[order]
+            if getattr(self, "_ids_dense", False):
+                # ids are the positions of the id order: one scatter per array
+                idx = cur.long()
+                res = {}
+                for k, v in out.items():
+                    res[k] = torch.empty_like(v).index_copy_(0, idx, v)
+                res["id"] = torch.arange(N, dtype=torch.int32, device=dev)
+                out = res
+            else:
+                order = torch.argsort(cur.long())
+                out = {k: v[order] for k, v in out.items()}
+                out["id"] = cur[order]
         return out
 
     def state_bytes(self):
