@@ -161,6 +161,37 @@ int pxrb_push_em3d_bvec(const int64_t* xlo, const int64_t* xhi, const int64_t* y
                         const int64_t* bzlo, const int64_t* bzhi, double dtsdx, double dtsdy,
                         double dtsdz, void* stream);
 
+/* Replaces pxrpush_em3d_evec_norder (yee.F90:46-123): E += arbitrary-order
+ * curl B - mudt J on nodes [-nxs, nx+nxs] x ... of nine arrays of shape
+ * (-guard:n+guard) per axis; dtsdx[norderx/2] ... are HOST arrays of the
+ * difference weights times c^2 dt / d (norder even, 2..32); l_nodalgrid != 0
+ * selects the nodal stencil.  Stencils are clipped where the arrays end,
+ * as in the reference. */
+int pxrb_push_em3d_evec_norder(double* ex, double* ey, double* ez, const double* bx,
+                               const double* by, const double* bz, const double* jx,
+                               const double* jy, const double* jz, double mudt,
+                               const double* dtsdx, const double* dtsdy, const double* dtsdz,
+                               int64_t nx, int64_t ny, int64_t nz, int64_t norderx,
+                               int64_t nordery, int64_t norderz, int64_t nxguard,
+                               int64_t nyguard, int64_t nzguard, int64_t nxs, int64_t nys,
+                               int64_t nzs, int64_t l_nodalgrid, void* stream);
+
+/* Replaces pxrpush_em3d_bvec_norder (yee.F90:752-821): B -= arbitrary-order
+ * curl E, same conventions (weights times dt / d, halved by the caller for a
+ * half step as push_bfield does). */
+int pxrb_push_em3d_bvec_norder(const double* ex, const double* ey, const double* ez,
+                               double* bx, double* by, double* bz, const double* dtsdx,
+                               const double* dtsdy, const double* dtsdz, int64_t nx, int64_t ny,
+                               int64_t nz, int64_t norderx, int64_t nordery, int64_t norderz,
+                               int64_t nxguard, int64_t nyguard, int64_t nzguard, int64_t nxs,
+                               int64_t nys, int64_t nzs, int64_t l_nodalgrid, void* stream);
+
+/* Replaces FD_weights (src/submain.F90:927-984): the norder/2 weights of
+ * the first derivative on the staggered (l_nodal = 0) or nodal grid, the
+ * reference's form of Fornberg's recursion.  Host function; coeffs: HOST
+ * double[norder/2]. */
+int pxrb_fd_weights(double* coeffs, int64_t norder, int64_t l_nodal);
+
 /* Replaces field_bc -> exchange_mpi_3d_grid_array_with_guards for a single
  * periodic domain (src/boundary_conditions/field_boundaries.F90:81-269), for
  * one to three grids of the same shape (f2/f3 may be NULL).  Needs n > g. */
@@ -178,6 +209,23 @@ int pxrb_summation_bcs_periodic(double* f1, double* f2, double* f3, int64_t nx, 
 int pxrb_particle_bcs_periodic(int64_t np, double* xp, double* yp, double* zp, double xmin,
                                double ymin, double zmin, double xmax, double ymax,
                                double zmax, void* stream);
+
+/* Replaces the per-side pbound cases of particle_bcs for one domain
+ * (src/boundary_conditions/particle_boundaries.F90:1098-1300): pbound (HOST
+ * int64[6]: x-, x+, y-, y+, z-, z+) 0 periodic, 1 absorbing (particle
+ * removed), 2 reflecting (moved one cell in, u negated), 3 reinjecting
+ * (mirrored, u = 0, clamped into the tile region tile_lo..tile_hi (HOST
+ * double[3] each) less half a cell).  Removed particles are compacted out,
+ * keeping the survivors' order; every array among xp..uzp, gaminv, w and pid
+ * (the last three optional) is compacted.  np_out: DEVICE int64, the number
+ * left.  scratch: DEVICE bytes >= pxrb_particle_bcs_scratch(np). */
+int64_t pxrb_particle_bcs_scratch(int64_t np);
+int pxrb_particle_bcs(int64_t np, double* xp, double* yp, double* zp, double* uxp, double* uyp,
+                      double* uzp, double* gaminv, double* w, double* pid, double xmin_part,
+                      double ymin_part, double zmin_part, double xmax_part, double ymax_part,
+                      double zmax_part, double dx, double dy, double dz, const int64_t* pbound,
+                      const double* tile_lo, const double* tile_hi, void* scratch,
+                      int64_t scratch_bytes, int64_t* np_out, void* stream);
 
 /* Replaces pxr_particle_bin_sorting (src/housekeeping/sorting.F90:247-361):
  * particles reordered by bin number iz*nx3*ny3 + iy*nx3 + ix, with

@@ -46,7 +46,10 @@ ROUTINES = [
     ("particle_deposition/current_deposition/esirkepov/esirkepov_3d.F90",
      [f"depose_jxjyjz_esirkepov_{o}_{o}_{o}" for o in (1, 2, 3)]
      + ["pxr_depose_jxjyjz_esirkepov_n"]),
-    ("field_solvers/Maxwell/yee_solver/yee.F90", ["pxrpush_em3d_evec", "pxrpush_em3d_bvec"]),
+    ("field_solvers/Maxwell/yee_solver/yee.F90",
+     ["pxrpush_em3d_evec", "pxrpush_em3d_bvec", "pxrpush_em3d_evec_norder",
+      "pxrpush_em3d_bvec_norder"]),
+    ("submain.F90", ["FD_weights"]),
     ("field_gathering/energy_conserving/field_gathering_o1_3d.F90",
      ["gete3d_energy_conserving_scalar_1_1_1", "getb3d_energy_conserving_scalar_1_1_1"]),
     ("field_gathering/energy_conserving/field_gathering_o2_3d.F90",

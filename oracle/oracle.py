@@ -100,6 +100,11 @@ def _declare(L):
     L.orc_num_threads.restype = C.c_int
     L.orc_particle_bin_sorting.argtypes = [i64] + [P] * 8 + [f64] * 9
     L.orc_sim_get_particle_columns.argtypes = [vp, P, i64, P]
+    L.orc_pxrpush_em3d_evec_norder.argtypes = [P] * 9 + [f64, P, P, P] + [i64] * 13
+    L.orc_pxrpush_em3d_bvec_norder.argtypes = [P] * 6 + [P, P, P] + [i64] * 13
+    L.orc_FD_weights.argtypes = [P, i64, i64]
+    L.orc_particle_bcs.argtypes = [i64] + [P] * 9 + [P] * 4 + [P, P]
+    L.orc_particle_bcs.restype = i64
 
 
 def _c(a):
@@ -132,6 +137,41 @@ def set_gamma(ux, uy, uz, gaminv, clight=1.0):
 
 def pushxyz(x, y, z, ux, uy, uz, gaminv, dt):
     lib().orc_pushxyz(len(x), _p(x), _p(y), _p(z), _p(ux), _p(uy), _p(uz), _p(gaminv), dt)
+
+
+def particle_bcs(x, y, z, ux, uy, uz, gi, w, ids, lo, hi, d, pbound, tlo, thi):
+    """particle_bcs of one domain with per-side codes (in place); returns the
+    number of particles left (the first n entries of every array)."""
+    v = [np.ascontiguousarray(a, dtype=np.float64) for a in (lo, hi, d, tlo, thi)]
+    pb = np.ascontiguousarray(pbound, dtype=np.int64)
+    return lib().orc_particle_bcs(len(x), _p(x), _p(y), _p(z), _p(ux), _p(uy), _p(uz), _p(gi),
+                                  _p(w), _p(ids), _p(v[0]), _p(v[1]), _p(v[2]), _p(pb),
+                                  _p(v[3]), _p(v[4]))
+
+
+def fd_weights(norder, nodal=False):
+    """FD_weights: the norder/2 first-derivative weights."""
+    c = np.zeros(max(norder // 2, 1), dtype=np.float64)
+    lib().orc_FD_weights(_p(c), norder, int(bool(nodal)))
+    return c[:norder // 2]
+
+
+def push_em3d_evec_norder(ex, ey, ez, bx, by, bz, jx, jy, jz, mudt, dtsdx, dtsdy, dtsdz, n,
+                          norder, g, nodal=False, ns=(0, 0, 0)):
+    """pxrpush_em3d_evec_norder on Fortran-ordered (-g:n+g)^3 grids, in place."""
+    c = [np.ascontiguousarray(v, dtype=np.float64) for v in (dtsdx, dtsdy, dtsdz)]
+    lib().orc_pxrpush_em3d_evec_norder(*[_p(a) for a in (ex, ey, ez, bx, by, bz, jx, jy, jz)],
+                                       mudt, *[_p(a) for a in c], *n, *norder, g, g, g, *ns,
+                                       int(bool(nodal)))
+
+
+def push_em3d_bvec_norder(ex, ey, ez, bx, by, bz, dtsdx, dtsdy, dtsdz, n, norder, g,
+                          nodal=False, ns=(0, 0, 0)):
+    """pxrpush_em3d_bvec_norder on Fortran-ordered (-g:n+g)^3 grids, in place."""
+    c = [np.ascontiguousarray(v, dtype=np.float64) for v in (dtsdx, dtsdy, dtsdz)]
+    lib().orc_pxrpush_em3d_bvec_norder(*[_p(a) for a in (ex, ey, ez, bx, by, bz)],
+                                       *[_p(a) for a in c], *n, *norder, g, g, g, *ns,
+                                       int(bool(nodal)))
 
 
 def particle_bin_sorting(x, y, z, ux, uy, uz, gam, w, lo, hi, dbin):

@@ -1051,6 +1051,207 @@ void orc_depose_rho_scalar(i64 order, double* rho_, i64 np, const double* xp,
 // bnds: [xlo(3) xhi(3) ylo(3) yhi(3) zlo(3) zhi(3)]; alo/ahi: 9 (E) or 6 (B)
 // arrays' bounds, 3 each, in argument order ex,ey,ez,bx,by,bz,jx,jy,jz.
 // ----------------------------------------------------------------------------
+// ----------------------------------------------------------------------------
+// Arbitrary-order Yee pushes, yee.F90:46-123 (E) and :752-821 (B): for each
+// node of [-nxs, nx+nxs] x ..., the sum over i = 1..min(norder/2, distance to
+// the array's upper and lower ends) of dtsd(i) times the difference of the
+// source field at +-i (staggered: ist = 1, the forward point shifted back by
+// one for E, the backward one forward by one for B; nodal grid: ist = 0).
+// All nine arrays (-guard:n+guard) per axis; dtsdx(norderx/2) etc.
+// ----------------------------------------------------------------------------
+static inline i64 nord_hi(i64 half, i64 n, i64 g, i64 j) {
+  return std::min(std::min(half, (n - j) + g), j + g);
+}
+
+void orc_pxrpush_em3d_evec_norder(double* ex_, double* ey_, double* ez_, double* bx_,
+                                  double* by_, double* bz_, double* jx_, double* jy_,
+                                  double* jz_, double mudt, const double* dtsdx,
+                                  const double* dtsdy, const double* dtsdz, i64 nx, i64 ny,
+                                  i64 nz, i64 norderx, i64 nordery, i64 norderz, i64 nxguard,
+                                  i64 nyguard, i64 nzguard, i64 nxs, i64 nys, i64 nzs,
+                                  i64 l_nodalgrid) {
+  F3 Ex = gview(ex_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Ey = gview(ey_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Ez = gview(ez_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Bx = gview(bx_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 By = gview(by_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Bz = gview(bz_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Jx = gview(jx_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Jy = gview(jy_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Jz = gview(jz_, nx, ny, nz, nxguard, nyguard, nzguard);
+  const i64 ist = l_nodalgrid ? 0 : 1;
+#pragma omp parallel for schedule(static)
+  for (i64 l = -nzs; l <= nz + nzs; ++l)
+    for (i64 k = -nys; k <= ny + nys; ++k)
+      for (i64 j = -nxs; j <= nx + nxs; ++j) {
+        Ex(j, k, l) = Ex(j, k, l) - mudt * Jx(j, k, l);
+        for (i64 i = 1; i <= nord_hi(nordery / 2, ny, nyguard, k); ++i)
+          Ex(j, k, l) = Ex(j, k, l) + dtsdy[i - 1] * (Bz(j, k + i - ist, l) - Bz(j, k - i, l));
+        for (i64 i = 1; i <= nord_hi(norderz / 2, nz, nzguard, l); ++i)
+          Ex(j, k, l) = Ex(j, k, l) - dtsdz[i - 1] * (By(j, k, l + i - ist) - By(j, k, l - i));
+      }
+#pragma omp parallel for schedule(static)
+  for (i64 l = -nzs; l <= nz + nzs; ++l)
+    for (i64 k = -nys; k <= ny + nys; ++k)
+      for (i64 j = -nxs; j <= nx + nxs; ++j) {
+        Ey(j, k, l) = Ey(j, k, l) - mudt * Jy(j, k, l);
+        for (i64 i = 1; i <= nord_hi(norderx / 2, nx, nxguard, j); ++i)
+          Ey(j, k, l) = Ey(j, k, l) - dtsdx[i - 1] * (Bz(j + i - ist, k, l) - Bz(j - i, k, l));
+        for (i64 i = 1; i <= nord_hi(norderz / 2, nz, nzguard, l); ++i)
+          Ey(j, k, l) = Ey(j, k, l) + dtsdz[i - 1] * (Bx(j, k, l + i - ist) - Bx(j, k, l - i));
+      }
+#pragma omp parallel for schedule(static)
+  for (i64 l = -nzs; l <= nz + nzs; ++l)
+    for (i64 k = -nys; k <= ny + nys; ++k)
+      for (i64 j = -nxs; j <= nx + nxs; ++j) {
+        Ez(j, k, l) = Ez(j, k, l) - mudt * Jz(j, k, l);
+        for (i64 i = 1; i <= nord_hi(norderx / 2, nx, nxguard, j); ++i)
+          Ez(j, k, l) = Ez(j, k, l) + dtsdx[i - 1] * (By(j + i - ist, k, l) - By(j - i, k, l));
+        for (i64 i = 1; i <= nord_hi(nordery / 2, ny, nyguard, k); ++i)
+          Ez(j, k, l) = Ez(j, k, l) - dtsdy[i - 1] * (Bx(j, k + i - ist, l) - Bx(j, k - i, l));
+      }
+}
+
+void orc_pxrpush_em3d_bvec_norder(double* ex_, double* ey_, double* ez_, double* bx_,
+                                  double* by_, double* bz_, const double* dtsdx,
+                                  const double* dtsdy, const double* dtsdz, i64 nx, i64 ny,
+                                  i64 nz, i64 norderx, i64 nordery, i64 norderz, i64 nxguard,
+                                  i64 nyguard, i64 nzguard, i64 nxs, i64 nys, i64 nzs,
+                                  i64 l_nodalgrid) {
+  F3 Ex = gview(ex_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Ey = gview(ey_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Ez = gview(ez_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Bx = gview(bx_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 By = gview(by_, nx, ny, nz, nxguard, nyguard, nzguard);
+  F3 Bz = gview(bz_, nx, ny, nz, nxguard, nyguard, nzguard);
+  const i64 ist = l_nodalgrid ? 0 : 1;
+#pragma omp parallel for schedule(static)
+  for (i64 l = -nzs; l <= nz + nzs; ++l)
+    for (i64 k = -nys; k <= ny + nys; ++k)
+      for (i64 j = -nxs; j <= nx + nxs; ++j) {
+        for (i64 i = 1; i <= nord_hi(nordery / 2, ny, nyguard, k); ++i)
+          Bx(j, k, l) = Bx(j, k, l) - dtsdy[i - 1] * (Ez(j, k + i, l) - Ez(j, k - i + ist, l));
+        for (i64 i = 1; i <= nord_hi(norderz / 2, nz, nzguard, l); ++i)
+          Bx(j, k, l) = Bx(j, k, l) + dtsdz[i - 1] * (Ey(j, k, l + i) - Ey(j, k, l - i + ist));
+      }
+#pragma omp parallel for schedule(static)
+  for (i64 l = -nzs; l <= nz + nzs; ++l)
+    for (i64 k = -nys; k <= ny + nys; ++k)
+      for (i64 j = -nxs; j <= nx + nxs; ++j) {
+        for (i64 i = 1; i <= nord_hi(norderx / 2, nx, nxguard, j); ++i)
+          By(j, k, l) = By(j, k, l) + dtsdx[i - 1] * (Ez(j + i, k, l) - Ez(j - i + ist, k, l));
+        for (i64 i = 1; i <= nord_hi(norderz / 2, nz, nzguard, l); ++i)
+          By(j, k, l) = By(j, k, l) - dtsdz[i - 1] * (Ex(j, k, l + i) - Ex(j, k, l - i + ist));
+      }
+#pragma omp parallel for schedule(static)
+  for (i64 l = -nzs; l <= nz + nzs; ++l)
+    for (i64 k = -nys; k <= ny + nys; ++k)
+      for (i64 j = -nxs; j <= nx + nxs; ++j) {
+        for (i64 i = 1; i <= nord_hi(norderx / 2, nx, nxguard, j); ++i)
+          Bz(j, k, l) = Bz(j, k, l) - dtsdx[i - 1] * (Ey(j + i, k, l) - Ey(j - i + ist, k, l));
+        for (i64 i = 1; i <= nord_hi(nordery / 2, ny, nyguard, k); ++i)
+          Bz(j, k, l) = Bz(j, k, l) + dtsdy[i - 1] * (Ex(j, k + i, l) - Ex(j, k - i + ist, l));
+      }
+}
+
+// particle_bcs for one domain with per-side pbound codes
+// (particle_boundaries.F90:1098-1300): pb[6] = x-, x+, y-, y+, z-, z+;
+// 0 periodic, 1 absorbing, 2 reflecting, 3 reinjecting (see the cases
+// there); lo/hi: x_min_local_part ... (also xmin_part ... here), tlo/thi: the
+// tile particle region for the reinjection clamps.  Removal as
+// rm_particles_from_species_with_mask (tiling.F90:522-537): from the last
+// particle down, a removed one is replaced by the current last one.  Arrays
+// w and id may be NULL.  Returns the particle count left.
+i64 orc_particle_bcs(i64 np, double* x, double* y, double* z, double* ux, double* uy,
+                     double* uz, double* gi, double* w, double* id, const double* lo,
+                     const double* hi, const double* d, const i64* pb, const double* tlo,
+                     const double* thi) {
+  std::vector<char> mask(np, 1);
+  double* P[3] = {x, y, z};
+  double* U[3] = {ux, uy, uz};
+  for (i64 i = 0; i < np; ++i) {
+    bool done = false;
+    for (int a = 0; a < 3 && !done; ++a) {
+      const double part_xyz = P[a][i];
+      const double length = hi[a] - lo[a];
+      if (part_xyz < lo[a]) {
+        switch (pb[2 * a]) {
+          case 1: mask[i] = 0; done = true; break;
+          case 2: P[a][i] = part_xyz + d[a]; U[a][i] = -U[a][i]; break;
+          case 3:
+            P[a][i] = 2.0 * lo[a] - P[a][i];
+            ux[i] = 0.; uy[i] = 0.; uz[i] = 0.;
+            for (int b = 0; b < 3; ++b) {
+              P[b][i] = std::max(P[b][i], tlo[b] + 0.5 * d[b]);
+              P[b][i] = std::min(P[b][i], thi[b] - 0.5 * d[b]);
+            }
+            done = true;
+            break;
+          default: P[a][i] = part_xyz + length;
+        }
+      }
+      if (done) break;
+      if (part_xyz >= hi[a]) {
+        switch (pb[2 * a + 1]) {
+          case 1: mask[i] = 0; done = true; break;
+          case 2: P[a][i] = part_xyz - d[a]; U[a][i] = -U[a][i]; break;
+          case 3:
+            P[a][i] = 2.0 * hi[a] - P[a][i];
+            ux[i] = 0.; uy[i] = 0.; uz[i] = 0.;
+            for (int b = 0; b < 3; ++b) {
+              P[b][i] = std::max(P[b][i], tlo[b] + 0.5 * d[b]);
+              P[b][i] = std::min(P[b][i], thi[b] - 0.5 * d[b]);
+            }
+            done = true;
+            break;
+          default: P[a][i] = part_xyz - length;
+        }
+      }
+    }
+  }
+  double* cols[9] = {x, y, z, ux, uy, uz, gi, w, id};
+  i64 n = np;
+  for (i64 i = np - 1; i >= 0; --i) {
+    if (mask[i]) continue;
+    if (i != n - 1)
+      for (double* c : cols)
+        if (c) c[i] = c[n - 1];
+    n = n - 1;
+  }
+  return n;
+}
+
+// FD_weights (submain.F90:927-984): Fornberg's recursion for the weights of
+// the first derivative on norder+1 points x_i = i - n/2 + 1 at the point z
+// (0.5 on the staggered grid, 0 on the nodal one); coeffs(i) = c(1, n/2+i-1).
+void orc_FD_weights(double* coeffs, i64 norder, i64 l_nodal) {
+  const double z = l_nodal ? 0.0 : 0.5;
+  const i64 m = 1, n = norder + 1;
+  std::vector<double> x(n), c((m + 1) * n, 0.0);
+  auto C = [&](i64 k, i64 i) -> double& { return c[k + (m + 1) * i]; };
+  for (i64 i = 0; i <= n - 1; ++i) x[i] = (double)(i - n / 2 + 1);
+  double c1 = 1.0, c4 = x[0] - z;
+  C(0, 0) = 1.0;
+  for (i64 i = 1; i <= n - 1; ++i) {
+    const i64 mn = std::min(i + 1, m + 1);
+    double c2 = 1.0;
+    const double c5 = c4;
+    c4 = x[i] - z;
+    for (i64 j = 0; j <= i - 1; ++j) {
+      const double c3 = x[i] - x[j];
+      c2 = c2 * c3;
+      if (j == i - 1) {
+        for (i64 k = 1; k <= mn - 1; ++k) C(k, i) = c1 * (k * C(k - 1, i - 1) - c5 * C(k, i - 1)) / c2;
+        C(0, i) = -c1 * c5 * C(0, i - 1) / c2;
+        for (i64 k = 1; k <= mn - 1; ++k) C(k, j) = (c4 * C(k, j) - k * C(k - 1, j)) / c3;
+        C(0, j) = c4 * C(0, j) / c3;
+      }
+    }
+    c1 = c2;
+  }
+  for (i64 i = 1; i <= norder / 2; ++i) coeffs[i - 1] = C(m, norder / 2 + i - 1);
+}
+
 void orc_pxrpush_em3d_evec(const i64* bnds, double* ex_, double* ey_, double* ez_,
                            double* bx_, double* by_, double* bz_, double* jx_,
                            double* jy_, double* jz_, const i64* alo, const i64* ahi,

@@ -47,6 +47,11 @@ _SIGS = {
     "pxrb_particle_bcs_periodic": "i p p p" + " d" * 6 + " s",
     "pxrb_particle_bin_sorting": "i" + " p" * 8 + " d" * 9 + " p i s",
     "pxrb_particle_bin_sorting_scratch": "=i i",
+    "pxrb_push_em3d_evec_norder": "p" * 1 + " p" * 8 + " d p p p" + " i" * 13 + " s",
+    "pxrb_push_em3d_bvec_norder": "p" + " p" * 5 + " p p p" + " i" * 13 + " s",
+    "pxrb_fd_weights": "p i i",
+    "pxrb_particle_bcs_scratch": "=i i",
+    "pxrb_particle_bcs": "i" + " p" * 9 + " d" * 9 + " p p p p i p s",
 }
 for _o in (1, 2, 3):
     _SIGS[f"pxrb_field_gathering_plus_particle_pusher_{_o}_{_o}_{_o}"] = (

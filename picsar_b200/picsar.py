@@ -192,6 +192,10 @@ class PicsarModule:
                                                         + 1.0 / self.dz ** 2))
         self.dt = float(dt)
         self.nox = self.noy = self.noz = int(nox)
+        # Maxwell solver (modules.F90 fields): FDTD order per axis, nodal grid
+        self.norderx = self.nordery = self.norderz = 2
+        self.l_nodalgrid = False
+        self.nxs = self.nys = self.nzs = 0
         self.particle_pusher = int(particle_pusher)
         self.l_lower_order_in_v = True
         self.currdepo = 0
@@ -199,6 +203,12 @@ class PicsarModule:
         # particle sorting (shared_data, modules.F90:1491-1503): off by default
         # (control_file.F90:160-166); bin sizes in physical units, as after
         # the scaling by dx at start-up (submain.F90:601)
+        # particle boundaries per side (shared_data pbound_*): 0 periodic,
+        # 1 absorbing, 2 reflecting, 3 reinjecting
+        self.pbound_x_min = self.pbound_x_max = 0
+        self.pbound_y_min = self.pbound_y_max = 0
+        self.pbound_z_min = self.pbound_z_max = 0
+        self._bc_scratch = None
         self.sorting_activated = 0
         self.sorting_dx, self.sorting_dy, self.sorting_dz = self.dx, self.dy, self.dz
         self.sorting_shiftx = self.sorting_shifty = self.sorting_shiftz = 0.0
@@ -260,10 +270,50 @@ class PicsarModule:
                self.l_lower_order_in_v, dt=self.dt, particle_pusher=self.particle_pusher,
                clight=self.clight)
 
+    def _particle_bcs_general(self, sp, pb):
+        n = sp.np
+        need = _lib.query("pxrb_particle_bcs_scratch", n)
+        if self._bc_scratch is None or self._bc_scratch.numel() < need:
+            self._bc_scratch = torch.empty(need, dtype=torch.uint8, device=self.device)
+        nout = torch.empty(1, dtype=torch.int64, device=self.device)
+        pbh = np.ascontiguousarray(pb, dtype=np.int64)
+        # one tile spanning the domain: particle region [min - d/2, max)
+        # (tiling.F90:154-185), the bounds of the reinjection clamps
+        tlo = np.array([self.xmin - self.dx / 2, self.ymin - self.dy / 2,
+                        self.zmin - self.dz / 2])
+        thi = np.array([self.xmax, self.ymax, self.zmax])
+        _lib.call("pxrb_particle_bcs", n, _ptr(sp.part_x), _ptr(sp.part_y), _ptr(sp.part_z),
+                  _ptr(sp.part_ux), _ptr(sp.part_uy), _ptr(sp.part_uz), _ptr(sp.part_gaminv),
+                  _ptr(sp.pid_w), _ptr(sp.pid_id), self.xmin, self.ymin, self.zmin, self.xmax,
+                  self.ymax, self.zmax, self.dx, self.dy, self.dz, pbh.ctypes.data,
+                  tlo.ctypes.data, thi.ctypes.data, self._bc_scratch.data_ptr(),
+                  self._bc_scratch.numel(), nout.data_ptr(), _stream())
+        m = int(nout.item())
+        if m != n:
+            for c in ("part_x", "part_y", "part_z", "part_ux", "part_uy", "part_uz",
+                      "part_gaminv", "part_ex", "part_ey", "part_ez", "part_bx", "part_by",
+                      "part_bz", "pid_w", "pid_id"):
+                setattr(sp, c, getattr(sp, c)[:m])
+
+    def _pbounds(self):
+        return (self.pbound_x_min, self.pbound_x_max, self.pbound_y_min, self.pbound_y_max,
+                self.pbound_z_min, self.pbound_z_max)
+
     def particle_bcs(self):
-        """Periodic wrap of every species (particle_boundaries.F90:1109-1300).
-        Tiled engine: done by the fused particle kernel."""
+        """Particle boundaries of every species (particle_boundaries.F90:
+        1098-1300): the periodic wrap, or per side absorbing (removed),
+        reflecting or reinjecting particles.  Tiled engine: periodic only,
+        done by the fused particle kernel."""
+        pb = self._pbounds()
         if self._tiled is not None:
+            if any(pb):
+                raise PicsarB200Error("the tiled engine wraps particles periodically only; "
+                                      "use engine='plain' for other particle boundaries")
+            return
+        if any(pb):
+            for sp in self.species:
+                if sp.np:
+                    self._particle_bcs_general(sp, pb)
             return
         for sp in self.species:
             if sp.np == 0:
@@ -328,10 +378,30 @@ class PicsarModule:
             return
         _summation_bcs(self.rho, None, None, self.nx, self.ny, self.nz, self.nxjguards)
 
+    def _norder(self):
+        return (self.norderx, self.nordery, self.norderz) != (2, 2, 2)
+
+    def _fd_coeffs(self):
+        """xcoeffs, ycoeffs, zcoeffs of FD_weights (submain.F90:899-906)."""
+        return [FD_weights(np.zeros(o // 2), o, self.l_nodalgrid)
+                for o in (self.norderx, self.nordery, self.norderz)]
+
     def push_bfield(self):
-        """B half step, order-2 Yee (maxwell_solver_manager.F90:44-85)."""
+        """B half step (maxwell_solver_manager.F90:44-85): order-2 Yee, or the
+        arbitrary-order stencil when an norder is not 2."""
         if self._tiled is not None:
+            if self._norder():
+                raise PicsarB200Error("the tiled engine's Yee solver is order 2")
             self._tiled.push_b()
+            return
+        if self._norder():
+            cx, cy, cz = self._fd_coeffs()
+            pxrpush_em3d_bvec_norder(self.ex, self.ey, self.ez, self.bx, self.by, self.bz,
+                                     0.5 * self.dt / self.dx * cx, 0.5 * self.dt / self.dy * cy,
+                                     0.5 * self.dt / self.dz * cz, self.nx, self.ny, self.nz,
+                                     self.norderx, self.nordery, self.norderz, self.nxguards,
+                                     self.nyguards, self.nzguards, self.nxs, self.nys, self.nzs,
+                                     self.l_nodalgrid)
             return
         n = (self.nx, self.ny, self.nz)
         g = self.nxguards
@@ -348,7 +418,20 @@ class PicsarModule:
     def push_efield(self):
         """E full step (maxwell_solver_manager.F90:393-439)."""
         if self._tiled is not None:
+            if self._norder():
+                raise PicsarB200Error("the tiled engine's Yee solver is order 2")
             self._tiled.push_e()
+            return
+        if self._norder():
+            cx, cy, cz = self._fd_coeffs()
+            c2 = self.clight ** 2
+            pxrpush_em3d_evec_norder(self.ex, self.ey, self.ez, self.bx, self.by, self.bz,
+                                     self.jx, self.jy, self.jz, c2 * self.mu0 * self.dt,
+                                     c2 * self.dt / self.dx * cx, c2 * self.dt / self.dy * cy,
+                                     c2 * self.dt / self.dz * cz, self.nx, self.ny, self.nz,
+                                     self.norderx, self.nordery, self.norderz, self.nxguards,
+                                     self.nyguards, self.nzguards, self.nxs, self.nys, self.nzs,
+                                     self.l_nodalgrid)
             return
         n = (self.nx, self.ny, self.nz)
         g = self.nxguards
@@ -822,6 +905,52 @@ def pxrpush_em3d_bvec(xlo, xhi, ylo, yhi, zlo, zhi, ex, exlo, exhi, ey, eylo, ey
         args += [_ptr(arr, grid=True), p1, p2]
     _lib.call("pxrb_push_em3d_bvec", *args, float(dtsdx), float(dtsdy), float(dtsdz),
               _stream())
+
+
+def _host_f64(a, n, name):
+    v = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+    if v.size < n:
+        raise ValueError(f"{name}: needs {n} weights")
+    return v
+
+
+def pxrpush_em3d_evec_norder(ex, ey, ez, bx, by, bz, jx, jy, jz, mudt, dtsdx, dtsdy, dtsdz, nx,
+                             ny, nz, norderx, nordery, norderz, nxguard, nyguard, nzguard, nxs,
+                             nys, nzs, l_nodalgrid):
+    """yee.F90:46-123 (dtsdx ... host arrays of norder/2 weights)."""
+    w = [_host_f64(c, o // 2, nm) for c, o, nm in
+         ((dtsdx, norderx, "dtsdx"), (dtsdy, nordery, "dtsdy"), (dtsdz, norderz, "dtsdz"))]
+    _lib.call("pxrb_push_em3d_evec_norder",
+              *[_ptr(a, n, grid=True) for a, n in zip((ex, ey, ez, bx, by, bz, jx, jy, jz),
+                                                       ("ex", "ey", "ez", "bx", "by", "bz",
+                                                        "jx", "jy", "jz"))],
+              float(mudt), *[c.ctypes.data for c in w], int(nx), int(ny), int(nz),
+              int(norderx), int(nordery), int(norderz), int(nxguard), int(nyguard),
+              int(nzguard), int(nxs), int(nys), int(nzs), int(bool(l_nodalgrid)), _stream())
+
+
+def pxrpush_em3d_bvec_norder(ex, ey, ez, bx, by, bz, dtsdx, dtsdy, dtsdz, nx, ny, nz, norderx,
+                             nordery, norderz, nxguard, nyguard, nzguard, nxs, nys, nzs,
+                             l_nodalgrid):
+    """yee.F90:752-821 (dtsdx ... host arrays of norder/2 weights)."""
+    w = [_host_f64(c, o // 2, nm) for c, o, nm in
+         ((dtsdx, norderx, "dtsdx"), (dtsdy, nordery, "dtsdy"), (dtsdz, norderz, "dtsdz"))]
+    _lib.call("pxrb_push_em3d_bvec_norder",
+              *[_ptr(a, n, grid=True) for a, n in zip((ex, ey, ez, bx, by, bz),
+                                                       ("ex", "ey", "ez", "bx", "by", "bz"))],
+              *[c.ctypes.data for c in w], int(nx), int(ny), int(nz), int(norderx),
+              int(nordery), int(norderz), int(nxguard), int(nyguard), int(nzguard), int(nxs),
+              int(nys), int(nzs), int(bool(l_nodalgrid)), _stream())
+
+
+def FD_weights(coeffs, norder, l_nodal):
+    """submain.F90:927: fills coeffs (numpy float64, norder/2) in place and
+    returns it."""
+    c = np.asarray(coeffs)
+    if c.dtype != np.float64 or not c.flags.c_contiguous or c.size < norder // 2:
+        raise ValueError("coeffs: contiguous float64 array of norder/2 values")
+    _lib.call("pxrb_fd_weights", c.ctypes.data, int(norder), int(bool(l_nodal)))
+    return c
 
 
 def _check_bounds(arr, lo, hi):

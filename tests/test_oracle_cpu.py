@@ -263,3 +263,14 @@ def test_bin_sorting_is_a_stable_sort_by_bin():
     O.particle_bin_sorting(*got, lo, hi, d)
     for a, b in zip(got, want):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("norder", [2, 4, 6, 8, 16, 32])
+@pytest.mark.parametrize("nodal", [False, True])
+def test_library_fd_weights_match_oracle(norder, nodal):
+    """pxrb_fd_weights (a host function of the library, no GPU needed) gives
+    the oracle's FD_weights (itself pinned to the reference's routine) bit
+    for bit."""
+    from picsar_b200 import picsar as P
+    got = P.FD_weights(np.zeros(norder // 2), norder, nodal)
+    np.testing.assert_array_equal(got, O.fd_weights(norder, nodal))

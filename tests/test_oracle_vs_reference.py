@@ -225,6 +225,41 @@ def test_yee_evec_bvec():
         _eq(x, y, f"yee {c}")
 
 
+@pytest.mark.parametrize("norder", [2, 4, 6, 8, 12])
+@pytest.mark.parametrize("nodal", [False, True])
+def test_fd_weights(norder, nodal):
+    a = O.fd_weights(norder, nodal)
+    b = np.zeros(norder // 2)
+    R.call("FD_weights", R.arr(b), R.i64(norder), R.i64(int(nodal)))
+    _eq(a, b, f"FD_weights {norder} nodal={nodal}")
+
+
+@pytest.mark.parametrize("norder,nodal", [((4, 4, 4), False), ((6, 2, 8), False),
+                                          ((4, 6, 2), True)])
+def test_yee_norder(norder, nodal):
+    fa = _grids(810)
+    ja = _grids(811)[:3]
+    fb = [a.copy(order="F") for a in fa]
+    dts = [DT / d * O.fd_weights(o, nodal) for d, o in zip(D, norder)]
+    half = [0.5 * c for c in dts]
+    O.push_em3d_bvec_norder(*fa, *half, N, norder, G, nodal)
+    O.push_em3d_evec_norder(*fa, *ja, DT, *dts, N, norder, G, nodal)
+    O.push_em3d_bvec_norder(*fa, *half, N, norder, G, nodal)
+    ns = [R.i64(0)] * 3
+    gs = [R.i64(G)] * 3
+    args_n = [R.i64(v) for v in N] + [R.i64(o) for o in norder] + gs + ns + [R.i64(int(nodal))]
+    hb = [np.ascontiguousarray(c) for c in half]
+    db = [np.ascontiguousarray(c) for c in dts]
+    R.call("pxrpush_em3d_bvec_norder", *[R.arr(f) for f in fb], *[R.arr(c) for c in hb],
+           *args_n)
+    R.call("pxrpush_em3d_evec_norder", *[R.arr(f) for f in fb + ja], R.f64(DT),
+           *[R.arr(c) for c in db], *args_n)
+    R.call("pxrpush_em3d_bvec_norder", *[R.arr(f) for f in fb], *[R.arr(c) for c in hb],
+           *args_n)
+    for x, y, c in zip(fa, fb, ("ex", "ey", "ez", "bx", "by", "bz")):
+        _eq(x, y, f"yee norder {norder} {c}")
+
+
 def test_comparison_detects_one_ulp():
     """The harness is not vacuous: a one-ulp change of dt on the oracle side
     changes the Boris result, and the equality check reports it."""
