@@ -192,9 +192,71 @@ int pxrb_push_em3d_bvec_norder(const double* ex, const double* ey, const double*
  * double[norder/2]. */
 int pxrb_fd_weights(double* coeffs, int64_t norder, int64_t l_nodal);
 
+/* ------------------------------------------------------------------------
+ * 2D (x-z) path, plain FP64: grids are 2-D Fortran arrays (-guard:n+guard)
+ * in x and z (PICSAR's x-z arrays, ny = 0 with no y guards).
+ * ---------------------------------------------------------------------- */
+
+/* Replaces geteb2dxz_energy_conserving (src/field_gathering/
+ * field_gathering_manager_2d.F90:61-89 -> the scalar
+ * pxr_gete2dxz / pxr_getb2dxz_energy_conserving_scalar_{1_1,2_2,3_3},
+ * field_gathering_o{1,2,3}_2d.F90): accumulates into ex..bz; both
+ * l_lower_order_in_v branches and the nodal grid; nox = noz in 1..3; the y
+ * arguments are accepted and unused, as in the reference. */
+int pxrb_geteb2dxz_energy_conserving(
+    int64_t np, const double* xp, const double* yp, const double* zp, double* ex, double* ey,
+    double* ez, double* bx, double* by, double* bz, double xmin, double ymin, double zmin,
+    double dx, double dy, double dz, int64_t nx, int64_t ny, int64_t nz, int64_t nxguard,
+    int64_t nyguard, int64_t nzguard, int64_t nox, int64_t noy, int64_t noz,
+    const double* exg, const double* eyg, const double* ezg, const double* bxg,
+    const double* byg, const double* bzg, int64_t l4symtry, int64_t l_lower_order_in_v,
+    int64_t lvect, int64_t field_gathe_algo, int64_t l_nodal, void* stream);
+
+/* Replaces depose_jxjyjz_2d (src/particle_deposition/current_deposition/
+ * current_deposition_manager_2d.F90:42 -> pxr_depose_jxjyjz_esirkepov2d_
+ * {1_1,2_2,3_3}, esirkepov/esirkepov_2d.F90:452-1082): 2-D Esirkepov with
+ * the out-of-plane Jy, accumulating; nox = noz in 1..3. */
+int pxrb_depose_jxjyjz_2d(double* jx, double* jy, double* jz, int64_t np, const double* xp,
+                          const double* yp, const double* zp, const double* uxp,
+                          const double* uyp, const double* uzp, const double* gaminv,
+                          const double* w, double q, double xmin, double zmin, double dt,
+                          double dx, double dz, int64_t nx, int64_t nz, int64_t nxguard,
+                          int64_t nzguard, int64_t nox, int64_t noz, int64_t lvect,
+                          void* stream);
+
+/* Replace pxrpush_em2d_evec / pxrpush_em2d_bvec (yee.F90:216-310, :912-994);
+ * bounds: HOST int64[2] (x, z); dtsdy is accepted and unused. */
+int pxrb_push_em2d_evec(const int64_t* xlo, const int64_t* xhi, const int64_t* ylo,
+                        const int64_t* yhi, const int64_t* zlo, const int64_t* zhi,
+                        double* ex, const int64_t* exlo, const int64_t* exhi, double* ey,
+                        const int64_t* eylo, const int64_t* eyhi, double* ez,
+                        const int64_t* ezlo, const int64_t* ezhi, const double* bx,
+                        const int64_t* bxlo, const int64_t* bxhi, const double* by,
+                        const int64_t* bylo, const int64_t* byhi, const double* bz,
+                        const int64_t* bzlo, const int64_t* bzhi, const double* jx,
+                        const int64_t* jxlo, const int64_t* jxhi, const double* jy,
+                        const int64_t* jylo, const int64_t* jyhi, const double* jz,
+                        const int64_t* jzlo, const int64_t* jzhi, double mudt, double dtsdx,
+                        double dtsdy, double dtsdz, void* stream);
+int pxrb_push_em2d_bvec(const int64_t* xlo, const int64_t* xhi, const int64_t* ylo,
+                        const int64_t* yhi, const int64_t* zlo, const int64_t* zhi,
+                        const double* ex, const int64_t* exlo, const int64_t* exhi,
+                        const double* ey, const int64_t* eylo, const int64_t* eyhi,
+                        const double* ez, const int64_t* ezlo, const int64_t* ezhi,
+                        double* bx, const int64_t* bxlo, const int64_t* bxhi, double* by,
+                        const int64_t* bylo, const int64_t* byhi, double* bz,
+                        const int64_t* bzlo, const int64_t* bzhi, double dtsdx, double dtsdy,
+                        double dtsdz, void* stream);
+
+/* Replaces pxr_pushxz (src/particle_pushers/boris_pusher/boris_2d.F90:42). */
+int pxrb_pushxz(int64_t np, double* xp, double* zp, const double* uxp, const double* uzp,
+                const double* gaminv, double dt, void* stream);
+
 /* Replaces field_bc -> exchange_mpi_3d_grid_array_with_guards for a single
  * periodic domain (src/boundary_conditions/field_boundaries.F90:81-269), for
- * one to three grids of the same shape (f2/f3 may be NULL).  Needs n > g. */
+ * one to three grids of the same shape (f2/f3 may be NULL).  Needs n > g per
+ * axis, except an axis with n = 0 and g = 0 (the y axis of x-z grids), which
+ * is skipped. */
 int pxrb_field_bc_periodic(double* f1, double* f2, double* f3, int64_t nx, int64_t ny,
                            int64_t nz, int64_t nxg, int64_t nyg, int64_t nzg, void* stream);
 

@@ -48,8 +48,17 @@ ROUTINES = [
      + ["pxr_depose_jxjyjz_esirkepov_n"]),
     ("field_solvers/Maxwell/yee_solver/yee.F90",
      ["pxrpush_em3d_evec", "pxrpush_em3d_bvec", "pxrpush_em3d_evec_norder",
-      "pxrpush_em3d_bvec_norder"]),
+      "pxrpush_em3d_bvec_norder", "pxrpush_em2d_evec", "pxrpush_em2d_bvec"]),
     ("submain.F90", ["FD_weights"]),
+    ("field_gathering/energy_conserving/field_gathering_o1_2d.F90",
+     ["pxr_gete2dxz_energy_conserving_scalar_1_1", "pxr_getb2dxz_energy_conserving_scalar_1_1"]),
+    ("field_gathering/energy_conserving/field_gathering_o2_2d.F90",
+     ["pxr_gete2dxz_energy_conserving_scalar_2_2", "pxr_getb2dxz_energy_conserving_scalar_2_2"]),
+    ("field_gathering/energy_conserving/field_gathering_o3_2d.F90",
+     ["pxr_gete2dxz_energy_conserving_scalar_3_3", "pxr_getb2dxz_energy_conserving_scalar_3_3"]),
+    ("particle_deposition/current_deposition/esirkepov/esirkepov_2d.F90",
+     [f"pxr_depose_jxjyjz_esirkepov2d_{o}_{o}" for o in (1, 2, 3)]),
+    ("particle_pushers/boris_pusher/boris_2d.F90", ["pxr_pushxz"]),
     ("field_gathering/energy_conserving/field_gathering_o1_3d.F90",
      ["gete3d_energy_conserving_scalar_1_1_1", "getb3d_energy_conserving_scalar_1_1_1"]),
     ("field_gathering/energy_conserving/field_gathering_o2_3d.F90",
@@ -646,7 +655,11 @@ class Routine:
                 size.append(f"b_{n}_n{d}")
             out.append(f"  const int64_t b_{n}_size = {' * '.join(size)};")
             if not v.dummy:
+                # local arrays start at zero (gfortran -finit-local-zero): a
+                # routine that reads an element before setting it (the order-2
+                # 2-D Esirkepov reads sx0(+-2)) then has one defined meaning
                 out.append(f"  {v.ctype} v_{n}[b_{n}_size > 0 ? b_{n}_size : 1];")
+                out.append(f"  memset(v_{n}, 0, sizeof(v_{n}));")
         for n, v in self.vars.items():
             out.append(f"  (void)v_{n};")
         depth = 1

@@ -48,9 +48,9 @@ def _p(a):
         return None
     if a.dtype != np.float64 and a.dtype != np.int64:
         raise TypeError(f"oracle arrays must be float64/int64, got {a.dtype}")
-    if a.ndim == 3 and not a.flags.f_contiguous:
+    if a.ndim >= 2 and not a.flags.f_contiguous:
         raise ValueError("oracle grids must be Fortran-ordered (np.asfortranarray)")
-    if a.ndim != 3 and not a.flags.c_contiguous:
+    if a.ndim < 2 and not a.flags.c_contiguous:
         raise ValueError("oracle particle arrays must be contiguous")
     return a.ctypes.data_as(vp)
 
@@ -105,6 +105,15 @@ def _declare(L):
     L.orc_FD_weights.argtypes = [P, i64, i64]
     L.orc_particle_bcs.argtypes = [i64] + [P] * 9 + [P] * 4 + [P, P]
     L.orc_particle_bcs.restype = i64
+    L.orc_geteb2dxz_energy_conserving_scalar.argtypes = (
+        [i64, i64, P, P, P, P, P] + [f64] * 4 + [i64] * 5 + [P] * 3 + [i64, i64])
+    L.orc_depose_jxjyjz_esirkepov2d.argtypes = ([i64] + [P] * 3 + [i64] + [P] * 7 +
+                                                [f64] * 6 + [i64] * 4)
+    L.orc_pxrpush_em2d_evec.argtypes = [P] + [P] * 9 + [i64] * 3 + [f64] * 3
+    L.orc_pxrpush_em2d_bvec.argtypes = [P] + [P] * 6 + [i64] * 3 + [f64] * 2
+    L.orc_pushxz.argtypes = [i64] + [P] * 5 + [f64]
+    L.orc_field_bc_periodic_2d.argtypes = [P] + [i64] * 4
+    L.orc_summation_bcs_periodic_2d.argtypes = [P] + [i64] * 4
 
 
 def _c(a):
@@ -147,6 +156,50 @@ def particle_bcs(x, y, z, ux, uy, uz, gi, w, ids, lo, hi, d, pbound, tlo, thi):
     return lib().orc_particle_bcs(len(x), _p(x), _p(y), _p(z), _p(ux), _p(uy), _p(uz), _p(gi),
                                   _p(w), _p(ids), _p(v[0]), _p(v[1]), _p(v[2]), _p(pb),
                                   _p(v[3]), _p(v[4]))
+
+
+def zeros_grid2d(nx, nz, g):
+    """A 2-D (x-z) PICSAR grid (-g:n+g) per axis, Fortran order."""
+    return np.zeros((nx + 1 + 2 * g, nz + 1 + 2 * g), dtype=np.float64, order="F")
+
+
+def geteb2dxz(which, xp, zp, f1, f2, f3, xmin, zmin, dx, dz, n, g, order, g1, g2, g3,
+              lower=True, nodal=False):
+    """2-D energy-conserving gather (which 0: E, 1: B), accumulating."""
+    lib().orc_geteb2dxz_energy_conserving_scalar(
+        which, len(xp), _p(xp), _p(zp), _p(f1), _p(f2), _p(f3), xmin, zmin, dx, dz, n[0],
+        n[1], g, g, order, _p(g1), _p(g2), _p(g3), int(bool(lower)), int(bool(nodal)))
+
+
+def depose_jxjyjz_esirkepov2d(order, jx, jy, jz, x, z, ux, uy, uz, gi, w, q, xmin, zmin, dt,
+                              dx, dz, n, g):
+    lib().orc_depose_jxjyjz_esirkepov2d(order, _p(jx), _p(jy), _p(jz), len(x), _p(x), _p(z),
+                                        _p(ux), _p(uy), _p(uz), _p(gi), _p(w), q, xmin, zmin, dt,
+                                        dx, dz, n[0], n[1], g, g)
+
+
+def push_em2d_evec(ex, ey, ez, bx, by, bz, jx, jy, jz, n, g, mudt, dtsdx, dtsdz, bnds=None):
+    b = np.ascontiguousarray(bnds if bnds is not None else [0, 0, n[0], n[1]] * 3, dtype=np.int64)
+    lib().orc_pxrpush_em2d_evec(_p(b), *[_p(a) for a in (ex, ey, ez, bx, by, bz, jx, jy, jz)],
+                                n[0], n[1], g, mudt, dtsdx, dtsdz)
+
+
+def push_em2d_bvec(ex, ey, ez, bx, by, bz, n, g, dtsdx, dtsdz, bnds=None):
+    b = np.ascontiguousarray(bnds if bnds is not None else [0, 0, n[0], n[1]] * 3, dtype=np.int64)
+    lib().orc_pxrpush_em2d_bvec(_p(b), *[_p(a) for a in (ex, ey, ez, bx, by, bz)], n[0], n[1],
+                                g, dtsdx, dtsdz)
+
+
+def field_bc_2d(f, n, g):
+    lib().orc_field_bc_periodic_2d(_p(f), n[0], n[1], g, g)
+
+
+def summation_bcs_2d(f, n, g):
+    lib().orc_summation_bcs_periodic_2d(_p(f), n[0], n[1], g, g)
+
+
+def pushxz(x, z, ux, uz, gi, dt):
+    lib().orc_pushxz(len(x), _p(x), _p(z), _p(ux), _p(uz), _p(gi), dt)
 
 
 def fd_weights(norder, nodal=False):

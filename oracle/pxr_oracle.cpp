@@ -646,6 +646,202 @@ void orc_geteb3d_energy_conserving_scalar(
 }
 
 // ----------------------------------------------------------------------------
+// 2D (x-z) path.  Grids are 2-D Fortran arrays (-g:n+g) in x and z.
+// Gathers: pxr_gete2dxz / pxr_getb2dxz_energy_conserving_scalar_{1_1,2_2,3_3}
+// (src/field_gathering/energy_conserving/field_gathering_o{1,2,3}_2d.F90),
+// the 3-D scalar forms without the y axis: components summed as
+//   f(ip) += s_x(jj)*s_z(ll)*g(...) over (ll, jj).
+// E: Ex (stag x, node z), Ey (node, node), Ez (node x, stag z); B: Bx (node
+// x, stag z), By (stag, stag), Bz (stag x, node z).
+// ----------------------------------------------------------------------------
+struct F2 {
+  double* p;
+  i64 gx, gz, sx;
+  double& operator()(i64 i, i64 k) const { return p[(i + gx) + sx * (k + gz)]; }
+};
+inline F2 gview2(double* p, i64 nx, i64 nz, i64 gx, i64 gz) {
+  F2 f;
+  f.p = p; f.gx = gx; f.gz = gz; f.sx = nx + 1 + 2 * gx;
+  (void)nz;
+  return f;
+}
+
+inline double gather2(const F2& g, const Shape& a, const Shape& c, double acc) {
+  for (int ll = c.lo; ll <= c.hi; ++ll)
+    for (int jj = a.lo; jj <= a.hi; ++jj)
+      acc = acc + a.s[jj - a.lo] * c.s[ll - c.lo] * g(a.i0 + jj, c.i0 + ll);
+  return acc;
+}
+
+extern "C" {
+
+// which: 0 = E, 1 = B.  Accumulates into f1, f2, f3.
+void orc_geteb2dxz_energy_conserving_scalar(i64 which, i64 np, const double* xp,
+                                            const double* zp, double* f1, double* f2,
+                                            double* f3, double xmin, double zmin, double dx,
+                                            double dz, i64 nx, i64 nz, i64 nxguard,
+                                            i64 nzguard, i64 order, double* g1_, double* g2_,
+                                            double* g3_, i64 l_lower_order_in_v, i64 l_nodal) {
+  F2 g1 = gview2(g1_, nx, nz, nxguard, nzguard), g2 = gview2(g2_, nx, nz, nxguard, nzguard),
+     g3 = gview2(g3_, nx, nz, nxguard, nzguard);
+  const double ss = l_nodal ? 0.0 : 0.5;
+  const bool lower = l_lower_order_in_v != 0;
+  const double dxi = 1.0 / dx, dzi = 1.0 / dz;
+  for (i64 ip = 0; ip < np; ++ip) {
+    const double x = (xp[ip] - xmin) * dxi, z = (zp[ip] - zmin) * dzi;
+    Shape nxs, nzs, sxs, szs;
+    node_shape((int)order, x, nxs); node_shape((int)order, z, nzs);
+    stag_shape((int)order, lower, ss, x, sxs); stag_shape((int)order, lower, ss, z, szs);
+    if (which == 0) {
+      f1[ip] = gather2(g1, sxs, nzs, f1[ip]);
+      f2[ip] = gather2(g2, nxs, nzs, f2[ip]);
+      f3[ip] = gather2(g3, nxs, szs, f3[ip]);
+    } else {
+      f1[ip] = gather2(g1, nxs, szs, f1[ip]);
+      f2[ip] = gather2(g2, sxs, szs, f2[ip]);
+      f3[ip] = gather2(g3, sxs, nzs, f3[ip]);
+    }
+  }
+}
+
+// pxr_depose_jxjyjz_esirkepov2d_{1_1,2_2,3_3} (esirkepov_2d.F90:452-623,
+// :666-842, :843-1082), with l_particles_weight and no RZ or symmetry
+// options: new shape sx0 at x, old shape sx at xold = x - dt/dx*vx shifted by
+// the node difference; Jx prefix-summed along x inside each z row, Jz along z
+// per x column, Jy deposited directly (the 2-D Esirkepov out-of-plane
+// current).  The shape constants 1/6, 2/3 and the 1/3 of Jy are the
+// reference's default-real (single precision) values.
+void orc_depose_jxjyjz_esirkepov2d(i64 order, double* jx_, double* jy_, double* jz_, i64 np,
+                                   const double* xp, const double* zp, const double* uxp,
+                                   const double* uyp, const double* uzp, const double* gaminv,
+                                   const double* w, double q, double xmin, double zmin,
+                                   double dt, double dx, double dz, i64 nx, i64 nz,
+                                   i64 nxguard, i64 nzguard) {
+  F2 jx = gview2(jx_, nx, nz, nxguard, nzguard), jy = gview2(jy_, nx, nz, nxguard, nzguard),
+     jz = gview2(jz_, nx, nz, nxguard, nzguard);
+  const double onesixth_r = (double)(1.0f / 6.0f), twothird_r = (double)(2.0f / 3.0f);
+  const double onethird_r = (double)(1.0f / 3.0f);
+  const double dxi = 1.0 / dx, dzi = 1.0 / dz;
+  const double dtsdx0 = dt * dxi, dtsdz0 = dt * dzi;
+  const double invvol = 1.0 / (dx * dz), invdtdx = 1.0 / (dt * dz), invdtdz = 1.0 / (dt * dx);
+  // (-2:3) arrays at offset +2
+  double sx_[6], sz_[6], sx0_[6], sz0_[6], dsx_[6], dsz_[6], sdzk_[6], sdzkm1_[6];
+  double *sx = sx_ + 2, *sz = sz_ + 2, *sx0 = sx0_ + 2, *sz0 = sz0_ + 2, *dsx = dsx_ + 2,
+         *dsz = dsz_ + 2, *sdzk = sdzk_ + 2, *sdzkm1 = sdzkm1_ + 2;
+  for (int t = 0; t < 6; ++t) { sx0_[t] = sz0_[t] = sdzk_[t] = sdzkm1_[t] = 0.0; }
+  double sdxi = 0.0, sdxim1 = 0.0;
+  auto shape = [&](double xint, double* s, int off) {
+    if (order == 1) {
+      s[0 + off] = 1.0 - xint; s[1 + off] = xint;
+    } else if (order == 2) {
+      const double xs = xint * xint;
+      s[-1 + off] = 0.5 * (0.5 - xint) * (0.5 - xint);
+      s[0 + off] = 0.75 - xs;
+      s[1 + off] = 0.5 * (0.5 + xint) * (0.5 + xint);
+    } else {
+      const double ox = 1.0 - xint, xs = xint * xint, oxs = ox * ox;
+      s[-1 + off] = onesixth_r * oxs * ox;
+      s[0 + off] = twothird_r - xs * (1.0 - xint * 0.5);
+      s[1 + off] = twothird_r - oxs * (1.0 - ox * 0.5);
+      s[2 + off] = onesixth_r * xs * xint;
+    }
+  };
+  auto node = [&](double v) -> i64 { return order == 2 ? fnint(v) : ffloor(v); };
+  const int a = order == 1 ? 0 : 1, b = order == 3 ? 2 : 1;
+  for (i64 ip = 0; ip < np; ++ip) {
+    for (int t = 0; t < 6; ++t) { sx_[t] = sz_[t] = 0.0; }
+    if (order != 2) for (int t = 0; t < 6; ++t) { sx0_[t] = sz0_[t] = 0.0; }
+    const double x = (xp[ip] - xmin) * dxi, z = (zp[ip] - zmin) * dzi;
+    const double vx = uxp[ip] * gaminv[ip], vy = uyp[ip] * gaminv[ip],
+                 vz = uzp[ip] * gaminv[ip];
+    const double xold = x - dtsdx0 * vx, zold = z - dtsdz0 * vz;
+    const double wq = q * w[ip], wqx = wq * invdtdx, wqz = wq * invdtdz;
+    const i64 iixp0 = node(x), ikxp0 = node(z);
+    shape(x - iixp0, sx0, 0);
+    shape(z - ikxp0, sz0, 0);
+    const i64 iixp = node(xold), ikxp = node(zold);
+    const int dix = (int)(iixp - iixp0), diz = (int)(ikxp - ikxp0);
+    shape(xold - iixp, sx, dix);
+    shape(zold - ikxp, sz, diz);
+    for (int t = 0; t < 6; ++t) { dsx_[t] = sx_[t] - sx0_[t]; dsz_[t] = sz_[t] - sz0_[t]; }
+    const int ixmin = std::min(0, dix) - a, ixmax = std::max(0, dix) + b;
+    const int izmin = std::min(0, diz) - a, izmax = std::max(0, diz) + b;
+    for (int k = izmin; k <= izmax; ++k) {
+      for (int i = ixmin; i <= ixmax; ++i) {
+        const i64 ic = iixp0 + i, kc = ikxp0 + k;
+        if (i < ixmax) {
+          sdxi = wqx * dsx[i] * (sz0[k] + 0.5 * dsz[k]);
+          if (i > ixmin) sdxi = sdxi + sdxim1;
+          jx(ic, kc) = jx(ic, kc) + sdxi;
+        }
+        jy(ic, kc) = jy(ic, kc) + wq * vy * invvol *
+                                      ((sz0[k] + 0.5 * dsz[k]) * sx0[i] +
+                                       (0.5 * sz0[k] + onethird_r * dsz[k]) * dsx[i]);
+        if (k < izmax) {
+          sdzk[i] = wqz * dsz[k] * (sx0[i] + 0.5 * dsx[i]);
+          if (k > izmin) sdzk[i] = sdzk[i] + sdzkm1[i];
+          jz(ic, kc) = jz(ic, kc) + sdzk[i];
+        }
+        sdxim1 = sdxi;
+      }
+      for (int t = 0; t < 6; ++t) sdzkm1_[t] = sdzk_[t];
+    }
+  }
+}
+
+// pxrpush_em2d_evec / pxrpush_em2d_bvec (yee.F90:216-310, :912-994): the
+// order-2 Yee update in x-z; bnds: [xlo(2) xhi(2) ylo(2) yhi(2) zlo(2)
+// zhi(2)] loop ranges of the three components; every array (-g:n+g)^2.
+void orc_pxrpush_em2d_evec(const i64* bnds, double* ex_, double* ey_, double* ez_, double* bx_,
+                           double* by_, double* bz_, double* jx_, double* jy_, double* jz_,
+                           i64 nx, i64 nz, i64 g, double mudt, double dtsdx, double dtsdz) {
+  F2 Ex = gview2(ex_, nx, nz, g, g), Ey = gview2(ey_, nx, nz, g, g), Ez = gview2(ez_, nx, nz, g, g),
+     Bx = gview2(bx_, nx, nz, g, g), By = gview2(by_, nx, nz, g, g), Bz = gview2(bz_, nx, nz, g, g),
+     Jx = gview2(jx_, nx, nz, g, g), Jy = gview2(jy_, nx, nz, g, g), Jz = gview2(jz_, nx, nz, g, g);
+  const i64 *xlo = bnds, *xhi = bnds + 2, *ylo = bnds + 4, *yhi = bnds + 6, *zlo = bnds + 8,
+            *zhi = bnds + 10;
+  for (i64 k = xlo[1]; k <= xhi[1]; ++k)
+    for (i64 j = xlo[0]; j <= xhi[0]; ++j)
+      Ex(j, k) = Ex(j, k) - dtsdz * (By(j, k) - By(j, k - 1)) - mudt * Jx(j, k);
+  for (i64 k = ylo[1]; k <= yhi[1]; ++k)
+    for (i64 j = ylo[0]; j <= yhi[0]; ++j)
+      Ey(j, k) = Ey(j, k) - dtsdx * (Bz(j, k) - Bz(j - 1, k)) + dtsdz * (Bx(j, k) - Bx(j, k - 1)) -
+                 mudt * Jy(j, k);
+  for (i64 k = zlo[1]; k <= zhi[1]; ++k)
+    for (i64 j = zlo[0]; j <= zhi[0]; ++j)
+      Ez(j, k) = Ez(j, k) + dtsdx * (By(j, k) - By(j - 1, k)) - mudt * Jz(j, k);
+}
+
+void orc_pxrpush_em2d_bvec(const i64* bnds, double* ex_, double* ey_, double* ez_, double* bx_,
+                           double* by_, double* bz_, i64 nx, i64 nz, i64 g, double dtsdx,
+                           double dtsdz) {
+  F2 Ex = gview2(ex_, nx, nz, g, g), Ey = gview2(ey_, nx, nz, g, g), Ez = gview2(ez_, nx, nz, g, g),
+     Bx = gview2(bx_, nx, nz, g, g), By = gview2(by_, nx, nz, g, g), Bz = gview2(bz_, nx, nz, g, g);
+  const i64 *xlo = bnds, *xhi = bnds + 2, *ylo = bnds + 4, *yhi = bnds + 6, *zlo = bnds + 8,
+            *zhi = bnds + 10;
+  for (i64 k = xlo[1]; k <= xhi[1]; ++k)
+    for (i64 j = xlo[0]; j <= xhi[0]; ++j)
+      Bx(j, k) = Bx(j, k) + dtsdz * (Ey(j, k + 1) - Ey(j, k));
+  for (i64 k = ylo[1]; k <= yhi[1]; ++k)
+    for (i64 j = ylo[0]; j <= yhi[0]; ++j)
+      By(j, k) = By(j, k) + dtsdx * (Ez(j + 1, k) - Ez(j, k)) - dtsdz * (Ex(j, k + 1) - Ex(j, k));
+  for (i64 k = zlo[1]; k <= zhi[1]; ++k)
+    for (i64 j = zlo[0]; j <= zhi[0]; ++j)
+      Bz(j, k) = Bz(j, k) - dtsdx * (Ey(j + 1, k) - Ey(j, k));
+}
+
+// pxr_pushxz (boris_2d.F90:42-60)
+void orc_pushxz(i64 np, double* xp, double* zp, const double* uxp, const double* uzp,
+                const double* gaminv, double dt) {
+  for (i64 ip = 0; ip < np; ++ip) {
+    xp[ip] = xp[ip] + uxp[ip] * gaminv[ip] * dt;
+    zp[ip] = zp[ip] + uzp[ip] * gaminv[ip] * dt;
+  }
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------
 // Esirkepov current deposition (accumulates into jx, jy, jz).
 // src/particle_deposition/current_deposition/esirkepov/esirkepov_3d.F90:
 //   depose_jxjyjz_esirkepov_1_1_1  :82-239
@@ -1365,6 +1561,30 @@ void orc_summation_bcs_periodic(double* f, i64 nx, i64 ny, i64 nz, i64 nxg, i64 
     slab_copy(a, ax, -g[ax], n[ax] - g[ax], g[ax] + 1, elo, ehi, true);
   }
   orc_field_bc_periodic(f, nx, ny, nz, nxg, nyg, nzg);
+}
+
+// c_dim = 2 (x-z arrays, ny = 0, no y guards): the same exchanges along x and
+// z only; the reference skips the y exchange there (field_boundaries.F90:330,
+// :444).
+void orc_field_bc_periodic_2d(double* f, i64 nx, i64 nz, i64 nxg, i64 nzg) {
+  F3 a = gview(f, nx, 0, nz, nxg, 0, nzg);
+  const i64 n[3] = {nx, 0, nz}, g[3] = {nxg, 0, nzg};
+  const i64 elo[3] = {-nxg, 0, -nzg}, ehi[3] = {nx + nxg, 0, nz + nzg};
+  for (int ax = 0; ax < 3; ax += 2) {
+    slab_copy(a, ax, 0, n[ax], g[ax] + 1, elo, ehi, false);
+    slab_copy(a, ax, n[ax] - g[ax], -g[ax], g[ax] + 1, elo, ehi, false);
+  }
+}
+
+void orc_summation_bcs_periodic_2d(double* f, i64 nx, i64 nz, i64 nxg, i64 nzg) {
+  F3 a = gview(f, nx, 0, nz, nxg, 0, nzg);
+  const i64 n[3] = {nx, 0, nz}, g[3] = {nxg, 0, nzg};
+  const i64 elo[3] = {-nxg, 0, -nzg}, ehi[3] = {nx + nxg, 0, nz + nzg};
+  for (int ax = 0; ax < 3; ax += 2) {
+    slab_copy(a, ax, n[ax], 0, g[ax] + 1, elo, ehi, true);
+    slab_copy(a, ax, -g[ax], n[ax] - g[ax], g[ax] + 1, elo, ehi, true);
+  }
+  orc_field_bc_periodic_2d(f, nx, nz, nxg, nzg);
 }
 
 // ----------------------------------------------------------------------------

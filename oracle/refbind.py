@@ -61,9 +61,9 @@ def f64(v):
 def arr(a, dtype=np.float64):
     if a.dtype != dtype:
         raise TypeError(f"expected {dtype}, got {a.dtype}")
-    if a.ndim == 3 and not a.flags.f_contiguous:
+    if a.ndim >= 2 and not a.flags.f_contiguous:
         raise ValueError("grids must be Fortran-ordered")
-    if a.ndim != 3 and not a.flags.c_contiguous:
+    if a.ndim < 2 and not a.flags.c_contiguous:
         raise ValueError("arrays must be contiguous")
     return a.ctypes.data_as(C.c_void_p)
 

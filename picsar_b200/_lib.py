@@ -51,6 +51,12 @@ _SIGS = {
     "pxrb_push_em3d_bvec_norder": "p" + " p" * 5 + " p p p" + " i" * 13 + " s",
     "pxrb_fd_weights": "p i i",
     "pxrb_particle_bcs_scratch": "=i i",
+    "pxrb_geteb2dxz_energy_conserving": "i" + " p" * 9 + " d" * 6 + " i" * 9 + " p" * 6
+    + " i i i i i s",
+    "pxrb_depose_jxjyjz_2d": "p p p i" + " p" * 8 + " d" * 6 + " i" * 7 + " s",
+    "pxrb_push_em2d_evec": " p" * 6 + " p p p" * 9 + " d d d d s",
+    "pxrb_push_em2d_bvec": " p" * 6 + " p p p" * 6 + " d d d s",
+    "pxrb_pushxz": "i p p p p p d s",
     "pxrb_particle_bcs": "i" + " p" * 9 + " d" * 9 + " p p p p i p s",
 }
 for _o in (1, 2, 3):

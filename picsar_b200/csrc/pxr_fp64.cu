@@ -553,6 +553,212 @@ inline int grid_stride_blocks(i64 n) {
 
 bool bad_ptr(const void* p) { return p == nullptr; }
 
+// ---------------------------------------------------------------------------
+// 2D (x-z) path on PICSAR's 2-D arrays (-g:n+g) in x and z, Fortran order:
+// the separate energy-conserving gather (field_gathering_o{1,2,3}_2d.F90),
+// Esirkepov deposition (esirkepov_2d.F90:452-1082) with global FP64 atomics,
+// the order-2 Yee update (yee.F90:216-310, :912-994) and pxr_pushxz.
+// ---------------------------------------------------------------------------
+struct G2 {
+  i64 gx, gz, sx;
+  __device__ __forceinline__ i64 idx(i64 i, i64 k) const { return (i + gx) + sx * (k + gz); }
+};
+
+__device__ __forceinline__ double gsum2(const double* g, const G2& G, const Sh& a, const Sh& c,
+                                        double f) {
+  for (int ll = 0; ll < c.n; ++ll)
+    for (int jj = 0; jj < a.n; ++jj)
+      f = f + a.s[jj] * c.s[ll] * __ldg(g + G.idx(a.i0 + jj, c.i0 + ll));
+  return f;
+}
+
+struct GEB2Params {
+  i64 np;
+  const double *xp, *zp;
+  double *ex, *ey, *ez, *bx, *by, *bz;
+  double xmin, zmin, dxi, dzi;
+  const double *exg, *eyg, *ezg, *bxg, *byg, *bzg;
+  G2 G;
+  int order, lower;
+  double ss;
+};
+
+__global__ void __launch_bounds__(TPB) k_geteb2d(GEB2Params p) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < p.np;
+       i += (i64)gridDim.x * blockDim.x) {
+    const double x = (p.xp[i] - p.xmin) * p.dxi, z = (p.zp[i] - p.zmin) * p.dzi;
+    Sh nx, nz, sx, sz;
+    sh_node(p.order, x, nx); sh_node(p.order, z, nz);
+    sh_stag(p.order, p.lower, p.ss, x, sx); sh_stag(p.order, p.lower, p.ss, z, sz);
+    p.ex[i] = gsum2(p.exg, p.G, sx, nz, p.ex[i]);
+    p.ey[i] = gsum2(p.eyg, p.G, nx, nz, p.ey[i]);
+    p.ez[i] = gsum2(p.ezg, p.G, nx, sz, p.ez[i]);
+    p.bx[i] = gsum2(p.bxg, p.G, nx, sz, p.bx[i]);
+    p.by[i] = gsum2(p.byg, p.G, sx, sz, p.by[i]);
+    p.bz[i] = gsum2(p.bzg, p.G, sx, nz, p.bz[i]);
+  }
+}
+
+struct Dep2Params {
+  i64 np;
+  double *jx, *jy, *jz;
+  const double *xp, *zp, *uxp, *uyp, *uzp, *gaminv, *w;
+  double q, xmin, zmin, dt, dx, dz;
+  G2 G;
+};
+
+// The reference's 2-D shapes: order 3 with its default-real (single
+// precision) constants 1/6 and 2/3; array index off = shift of the shape.
+template <int ORDER>
+__device__ __forceinline__ void shape2d(double xint, double* s, int off) {
+  if (ORDER == 1) {
+    s[0 + off] = 1.0 - xint; s[1 + off] = xint;
+  } else if (ORDER == 2) {
+    const double xs = xint * xint;
+    s[-1 + off] = 0.5 * (0.5 - xint) * (0.5 - xint);
+    s[0 + off] = 0.75 - xs;
+    s[1 + off] = 0.5 * (0.5 + xint) * (0.5 + xint);
+  } else {
+    const double onesixth = (double)(1.0f / 6.0f), twothird = (double)(2.0f / 3.0f);
+    const double ox = 1.0 - xint, xs = xint * xint, oxs = ox * ox;
+    s[-1 + off] = onesixth * oxs * ox;
+    s[0 + off] = twothird - xs * (1.0 - xint * 0.5);
+    s[1 + off] = twothird - oxs * (1.0 - ox * 0.5);
+    s[2 + off] = onesixth * xs * xint;
+  }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(TPB) k_esirkepov2d(Dep2Params p) {
+  constexpr int a = ORDER == 1 ? 0 : 1, b = ORDER == 3 ? 2 : 1;
+  const double onethird = (double)(1.0f / 3.0f);
+  const double dxi = 1.0 / p.dx, dzi = 1.0 / p.dz;
+  const double dtsdx0 = p.dt * dxi, dtsdz0 = p.dt * dzi;
+  const double invvol = 1.0 / (p.dx * p.dz), invdtdx = 1.0 / (p.dt * p.dz),
+               invdtdz = 1.0 / (p.dt * p.dx);
+  for (i64 ip = blockIdx.x * (i64)blockDim.x + threadIdx.x; ip < p.np;
+       ip += (i64)gridDim.x * blockDim.x) {
+    // (-2:3) arrays at offset +2
+    double sx_[6] = {0, 0, 0, 0, 0, 0}, sz_[6] = {0, 0, 0, 0, 0, 0};
+    double sx0_[6] = {0, 0, 0, 0, 0, 0}, sz0_[6] = {0, 0, 0, 0, 0, 0};
+    double sdzk_[6] = {0, 0, 0, 0, 0, 0}, sdzkm1_[6] = {0, 0, 0, 0, 0, 0};
+    double *sx = sx_ + 2, *sz = sz_ + 2, *sx0 = sx0_ + 2, *sz0 = sz0_ + 2;
+    double *sdzk = sdzk_ + 2, *sdzkm1 = sdzkm1_ + 2;
+    const double x = (p.xp[ip] - p.xmin) * dxi, z = (p.zp[ip] - p.zmin) * dzi;
+    const double gi = p.gaminv[ip];
+    const double vx = p.uxp[ip] * gi, vy = p.uyp[ip] * gi, vz = p.uzp[ip] * gi;
+    const double xold = x - dtsdx0 * vx, zold = z - dtsdz0 * vz;
+    const double wq = p.q * p.w[ip], wqx = wq * invdtdx, wqz = wq * invdtdz;
+    const i64 iixp0 = ORDER == 2 ? (i64)round(x) : (i64)floor(x);
+    const i64 ikxp0 = ORDER == 2 ? (i64)round(z) : (i64)floor(z);
+    shape2d<ORDER>(x - iixp0, sx0, 0);
+    shape2d<ORDER>(z - ikxp0, sz0, 0);
+    const i64 iixp = ORDER == 2 ? (i64)round(xold) : (i64)floor(xold);
+    const i64 ikxp = ORDER == 2 ? (i64)round(zold) : (i64)floor(zold);
+    int dix = (int)(iixp - iixp0), diz = (int)(ikxp - ikxp0);
+    // a move of more than one cell per step (beyond the CFL limit) would
+    // leave the shape arrays: clamp, as no valid input reaches it
+    dix = dix < -1 ? -1 : (dix > 1 ? 1 : dix);
+    diz = diz < -1 ? -1 : (diz > 1 ? 1 : diz);
+    shape2d<ORDER>(xold - iixp, sx, dix);
+    shape2d<ORDER>(zold - ikxp, sz, diz);
+    const int ixmin = min(0, dix) - a, ixmax = max(0, dix) + b;
+    const int izmin = min(0, diz) - a, izmax = max(0, diz) + b;
+    double sdxi = 0.0, sdxim1 = 0.0;
+    for (int k = izmin; k <= izmax; ++k) {
+      const double dsz = sz[k] - sz0[k];
+      for (int i = ixmin; i <= ixmax; ++i) {
+        const double dsx = sx[i] - sx0[i];
+        const i64 c = p.G.idx(iixp0 + i, ikxp0 + k);
+        if (i < ixmax) {
+          sdxi = wqx * dsx * (sz0[k] + 0.5 * dsz);
+          if (i > ixmin) sdxi = sdxi + sdxim1;
+          atomicAdd(p.jx + c, sdxi);
+        }
+        atomicAdd(p.jy + c, wq * vy * invvol *
+                                ((sz0[k] + 0.5 * dsz) * sx0[i] + (0.5 * sz0[k] + onethird * dsz) * dsx));
+        if (k < izmax) {
+          sdzk[i] = wqz * dsz * (sx0[i] + 0.5 * dsx);
+          if (k > izmin) sdzk[i] = sdzk[i] + sdzkm1[i];
+          atomicAdd(p.jz + c, sdzk[i]);
+        }
+        sdxim1 = sdxi;
+      }
+      for (int t = 0; t < 6; ++t) sdzkm1_[t] = sdzk_[t];
+    }
+  }
+}
+
+struct Yee2Params {
+  double *ex, *ey, *ez, *bx, *by, *bz;
+  const double *jx, *jy, *jz;
+  G2 gex, gey, gez, gbx, gby, gbz, gjx, gjy, gjz;
+  int lo[3][2], hi[3][2];
+  int ulo[2], uhi[2];
+  double mudt, dtsdx, dtsdz;
+};
+
+__device__ __forceinline__ bool inr2(const int* lo, const int* hi, int j, int k) {
+  return j >= lo[0] && j <= hi[0] && k >= lo[1] && k <= hi[1];
+}
+
+__global__ void k_yee2d_e(Yee2Params p) {
+  const int j = p.ulo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = p.ulo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  if (j > p.uhi[0] || k > p.uhi[1]) return;
+  if (inr2(p.lo[0], p.hi[0], j, k)) {
+    double* e = p.ex + p.gex.idx(j, k);
+    *e = *e - p.dtsdz * (p.by[p.gby.idx(j, k)] - p.by[p.gby.idx(j, k - 1)]) -
+         p.mudt * p.jx[p.gjx.idx(j, k)];
+  }
+  if (inr2(p.lo[1], p.hi[1], j, k)) {
+    double* e = p.ey + p.gey.idx(j, k);
+    *e = *e - p.dtsdx * (p.bz[p.gbz.idx(j, k)] - p.bz[p.gbz.idx(j - 1, k)]) +
+         p.dtsdz * (p.bx[p.gbx.idx(j, k)] - p.bx[p.gbx.idx(j, k - 1)]) -
+         p.mudt * p.jy[p.gjy.idx(j, k)];
+  }
+  if (inr2(p.lo[2], p.hi[2], j, k)) {
+    double* e = p.ez + p.gez.idx(j, k);
+    *e = *e + p.dtsdx * (p.by[p.gby.idx(j, k)] - p.by[p.gby.idx(j - 1, k)]) -
+         p.mudt * p.jz[p.gjz.idx(j, k)];
+  }
+}
+
+__global__ void k_yee2d_b(Yee2Params p) {
+  const int j = p.ulo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = p.ulo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  if (j > p.uhi[0] || k > p.uhi[1]) return;
+  if (inr2(p.lo[0], p.hi[0], j, k)) {
+    double* b = p.bx + p.gbx.idx(j, k);
+    *b = *b + p.dtsdz * (p.ey[p.gey.idx(j, k + 1)] - p.ey[p.gey.idx(j, k)]);
+  }
+  if (inr2(p.lo[1], p.hi[1], j, k)) {
+    double* b = p.by + p.gby.idx(j, k);
+    *b = *b + p.dtsdx * (p.ez[p.gez.idx(j + 1, k)] - p.ez[p.gez.idx(j, k)]) -
+         p.dtsdz * (p.ex[p.gex.idx(j, k + 1)] - p.ex[p.gex.idx(j, k)]);
+  }
+  if (inr2(p.lo[2], p.hi[2], j, k)) {
+    double* b = p.bz + p.gbz.idx(j, k);
+    *b = *b - p.dtsdx * (p.ey[p.gey.idx(j + 1, k)] - p.ey[p.gey.idx(j, k)]);
+  }
+}
+
+__global__ void k_pushxz(i64 np, double* xp, double* zp, const double* uxp, const double* uzp,
+                         const double* gaminv, double dt) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < np;
+       i += (i64)gridDim.x * blockDim.x) {
+    xp[i] = xp[i] + uxp[i] * gaminv[i] * dt;
+    zp[i] = zp[i] + uzp[i] * gaminv[i] * dt;
+  }
+}
+
+inline G2 g2_lohi(const int64_t* lo, const int64_t* hi) {
+  G2 g;
+  g.gx = -lo[0]; g.gz = -lo[1];
+  g.sx = hi[0] - lo[0] + 1;
+  return g;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -852,13 +1058,17 @@ static int bc_launch(double** arrs, int na, int64_t nx, int64_t ny, int64_t nz, 
                      int64_t nyg, int64_t nzg, int mode, void* stream) {
   if (na < 1 || na > 3) return PXRB_EINVAL;
   for (int q = 0; q < na; ++q) if (!arrs[q]) return PXRB_EINVAL;
-  if (nx <= nxg || ny <= nyg || nz <= nzg || nxg < 0 || nyg < 0 || nzg < 0) return PXRB_ERANGE;
+  // an axis of no cells and no guards (ny = 0 of PICSAR's x-z grids) is skipped
+  auto bad = [](int64_t n, int64_t g) { return g < 0 || (n <= g && !(n == 0 && g == 0)); };
+  if (bad(nx, nxg) || bad(ny, nyg) || bad(nz, nzg)) return PXRB_ERANGE;
   BcParams p;
   for (int q = 0; q < 3; ++q) p.a[q] = q < na ? arrs[q] : nullptr;
   p.na = na; p.G = make_grid(nx, ny, nz, nxg, nyg, nzg); p.mode = mode;
   i64 ext[3] = {nx + 1 + 2 * nxg, ny + 1 + 2 * nyg, nz + 1 + 2 * nzg};
   cudaStream_t s = (cudaStream_t)stream;
+  const int64_t nn[3] = {nx, ny, nz}, gg[3] = {nxg, nyg, nzg};
   for (int ax = 0; ax < 3; ++ax) {
+    if (nn[ax] == 0 && gg[ax] == 0) continue;
     p.axis = ax;
     i64 nlines = ext[(ax + 1) % 3] * ext[(ax + 2) % 3];
     k_bc_axis<<<nblocks(nlines, 128), 128, 0, s>>>(p);
@@ -882,6 +1092,142 @@ int pxrb_summation_bcs_periodic(double* f1, double* f2, double* f3, int64_t nx, 
   int rc = bc_launch(a, na, nx, ny, nz, nxg, nyg, nzg, 1, stream);
   if (rc) return rc;
   return bc_launch(a, na, nx, ny, nz, nxg, nyg, nzg, 0, stream);
+}
+
+int pxrb_geteb2dxz_energy_conserving(
+    int64_t np, const double* xp, const double* yp, const double* zp, double* ex, double* ey,
+    double* ez, double* bx, double* by, double* bz, double xmin, double ymin, double zmin,
+    double dx, double dy, double dz, int64_t nx, int64_t ny, int64_t nz, int64_t nxguard,
+    int64_t nyguard, int64_t nzguard, int64_t nox, int64_t noy, int64_t noz,
+    const double* exg, const double* eyg, const double* ezg, const double* bxg,
+    const double* byg, const double* bzg, int64_t l4symtry, int64_t l_lower_order_in_v,
+    int64_t lvect, int64_t field_gathe_algo, int64_t l_nodal, void* stream) {
+  (void)yp; (void)ymin; (void)dy; (void)ny; (void)nyguard; (void)noy; (void)lvect;
+  (void)field_gathe_algo;
+  if (np < 0) return PXRB_EINVAL;
+  if (np == 0) return PXRB_OK;
+  if (nox != noz || nox < 1 || nox > 3 || l4symtry) return PXRB_EUNSUPPORTED;
+  if (!xp || !zp || !ex || !ey || !ez || !bx || !by || !bz || !exg || !eyg || !ezg || !bxg ||
+      !byg || !bzg)
+    return PXRB_EINVAL;
+  GEB2Params p;
+  p.np = np; p.xp = xp; p.zp = zp;
+  p.ex = ex; p.ey = ey; p.ez = ez; p.bx = bx; p.by = by; p.bz = bz;
+  p.xmin = xmin; p.zmin = zmin; p.dxi = 1.0 / dx; p.dzi = 1.0 / dz;
+  p.exg = exg; p.eyg = eyg; p.ezg = ezg; p.bxg = bxg; p.byg = byg; p.bzg = bzg;
+  p.G.gx = nxguard; p.G.gz = nzguard; p.G.sx = nx + 1 + 2 * nxguard;
+  p.order = (int)nox; p.lower = l_lower_order_in_v ? 1 : 0;
+  p.ss = l_nodal ? 0.0 : 0.5;
+  k_geteb2d<<<nblocks(np), TPB, 0, (cudaStream_t)stream>>>(p);
+  PXRB_CHECK_LAUNCH();
+  return PXRB_OK;
+}
+
+int pxrb_depose_jxjyjz_2d(double* jx, double* jy, double* jz, int64_t np, const double* xp,
+                          const double* yp, const double* zp, const double* uxp,
+                          const double* uyp, const double* uzp, const double* gaminv,
+                          const double* w, double q, double xmin, double zmin, double dt,
+                          double dx, double dz, int64_t nx, int64_t nz, int64_t nxguard,
+                          int64_t nzguard, int64_t nox, int64_t noz, int64_t lvect,
+                          void* stream) {
+  (void)yp; (void)lvect;
+  if (np < 0) return PXRB_EINVAL;
+  if (np == 0) return PXRB_OK;
+  if (nox != noz || nox < 1 || nox > 3) return PXRB_EUNSUPPORTED;
+  if (!jx || !jy || !jz || !xp || !zp || !uxp || !uyp || !uzp || !gaminv || !w)
+    return PXRB_EINVAL;
+  Dep2Params p;
+  p.np = np; p.jx = jx; p.jy = jy; p.jz = jz;
+  p.xp = xp; p.zp = zp; p.uxp = uxp; p.uyp = uyp; p.uzp = uzp; p.gaminv = gaminv; p.w = w;
+  p.q = q; p.xmin = xmin; p.zmin = zmin; p.dt = dt; p.dx = dx; p.dz = dz;
+  p.G.gx = nxguard; p.G.gz = nzguard; p.G.sx = nx + 1 + 2 * nxguard;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (nox == 1) k_esirkepov2d<1><<<nblocks(np), TPB, 0, s>>>(p);
+  else if (nox == 2) k_esirkepov2d<2><<<nblocks(np), TPB, 0, s>>>(p);
+  else k_esirkepov2d<3><<<nblocks(np), TPB, 0, s>>>(p);
+  PXRB_CHECK_LAUNCH();
+  return PXRB_OK;
+}
+
+static int yee2d_setup(Yee2Params& p, const int64_t* xlo, const int64_t* xhi, const int64_t* ylo,
+                       const int64_t* yhi, const int64_t* zlo, const int64_t* zhi) {
+  const int64_t* L[3] = {xlo, ylo, zlo};
+  const int64_t* H[3] = {xhi, yhi, zhi};
+  for (int a = 0; a < 2; ++a) { p.ulo[a] = 1 << 30; p.uhi[a] = -(1 << 30); }
+  for (int c = 0; c < 3; ++c)
+    for (int a = 0; a < 2; ++a) {
+      p.lo[c][a] = (int)L[c][a]; p.hi[c][a] = (int)H[c][a];
+      p.ulo[a] = p.lo[c][a] < p.ulo[a] ? p.lo[c][a] : p.ulo[a];
+      p.uhi[a] = p.hi[c][a] > p.uhi[a] ? p.hi[c][a] : p.uhi[a];
+    }
+  for (int a = 0; a < 2; ++a) if (p.uhi[a] < p.ulo[a]) return 1;
+  return 0;
+}
+
+int pxrb_push_em2d_evec(const int64_t* xlo, const int64_t* xhi, const int64_t* ylo,
+                        const int64_t* yhi, const int64_t* zlo, const int64_t* zhi,
+                        double* ex, const int64_t* exlo, const int64_t* exhi, double* ey,
+                        const int64_t* eylo, const int64_t* eyhi, double* ez,
+                        const int64_t* ezlo, const int64_t* ezhi, const double* bx,
+                        const int64_t* bxlo, const int64_t* bxhi, const double* by,
+                        const int64_t* bylo, const int64_t* byhi, const double* bz,
+                        const int64_t* bzlo, const int64_t* bzhi, const double* jx,
+                        const int64_t* jxlo, const int64_t* jxhi, const double* jy,
+                        const int64_t* jylo, const int64_t* jyhi, const double* jz,
+                        const int64_t* jzlo, const int64_t* jzhi, double mudt, double dtsdx,
+                        double dtsdy, double dtsdz, void* stream) {
+  (void)dtsdy;
+  if (!ex || !ey || !ez || !bx || !by || !bz || !jx || !jy || !jz) return PXRB_EINVAL;
+  Yee2Params p;
+  if (yee2d_setup(p, xlo, xhi, ylo, yhi, zlo, zhi)) return PXRB_OK;
+  p.ex = ex; p.ey = ey; p.ez = ez;
+  p.bx = const_cast<double*>(bx); p.by = const_cast<double*>(by); p.bz = const_cast<double*>(bz);
+  p.jx = jx; p.jy = jy; p.jz = jz;
+  p.gex = g2_lohi(exlo, exhi); p.gey = g2_lohi(eylo, eyhi); p.gez = g2_lohi(ezlo, ezhi);
+  p.gbx = g2_lohi(bxlo, bxhi); p.gby = g2_lohi(bylo, byhi); p.gbz = g2_lohi(bzlo, bzhi);
+  p.gjx = g2_lohi(jxlo, jxhi); p.gjy = g2_lohi(jylo, jyhi); p.gjz = g2_lohi(jzlo, jzhi);
+  p.mudt = mudt; p.dtsdx = dtsdx; p.dtsdz = dtsdz;
+  dim3 blk(32, 8, 1);
+  dim3 grd((p.uhi[0] - p.ulo[0] + 1 + 31) / 32, (p.uhi[1] - p.ulo[1] + 1 + 7) / 8, 1);
+  k_yee2d_e<<<grd, blk, 0, (cudaStream_t)stream>>>(p);
+  PXRB_CHECK_LAUNCH();
+  return PXRB_OK;
+}
+
+int pxrb_push_em2d_bvec(const int64_t* xlo, const int64_t* xhi, const int64_t* ylo,
+                        const int64_t* yhi, const int64_t* zlo, const int64_t* zhi,
+                        const double* ex, const int64_t* exlo, const int64_t* exhi,
+                        const double* ey, const int64_t* eylo, const int64_t* eyhi,
+                        const double* ez, const int64_t* ezlo, const int64_t* ezhi,
+                        double* bx, const int64_t* bxlo, const int64_t* bxhi, double* by,
+                        const int64_t* bylo, const int64_t* byhi, double* bz,
+                        const int64_t* bzlo, const int64_t* bzhi, double dtsdx, double dtsdy,
+                        double dtsdz, void* stream) {
+  (void)dtsdy;
+  if (!ex || !ey || !ez || !bx || !by || !bz) return PXRB_EINVAL;
+  Yee2Params p;
+  if (yee2d_setup(p, xlo, xhi, ylo, yhi, zlo, zhi)) return PXRB_OK;
+  p.ex = const_cast<double*>(ex); p.ey = const_cast<double*>(ey); p.ez = const_cast<double*>(ez);
+  p.bx = bx; p.by = by; p.bz = bz;
+  p.jx = p.jy = p.jz = nullptr;
+  p.gex = g2_lohi(exlo, exhi); p.gey = g2_lohi(eylo, eyhi); p.gez = g2_lohi(ezlo, ezhi);
+  p.gbx = g2_lohi(bxlo, bxhi); p.gby = g2_lohi(bylo, byhi); p.gbz = g2_lohi(bzlo, bzhi);
+  p.mudt = 0; p.dtsdx = dtsdx; p.dtsdz = dtsdz;
+  dim3 blk(32, 8, 1);
+  dim3 grd((p.uhi[0] - p.ulo[0] + 1 + 31) / 32, (p.uhi[1] - p.ulo[1] + 1 + 7) / 8, 1);
+  k_yee2d_b<<<grd, blk, 0, (cudaStream_t)stream>>>(p);
+  PXRB_CHECK_LAUNCH();
+  return PXRB_OK;
+}
+
+int pxrb_pushxz(int64_t np, double* xp, double* zp, const double* uxp, const double* uzp,
+                const double* gaminv, double dt, void* stream) {
+  if (np < 0) return PXRB_EINVAL;
+  if (np == 0) return PXRB_OK;
+  if (!xp || !zp || !uxp || !uzp || !gaminv) return PXRB_EINVAL;
+  k_pushxz<<<nblocks(np), TPB, 0, (cudaStream_t)stream>>>(np, xp, zp, uxp, uzp, gaminv, dt);
+  PXRB_CHECK_LAUNCH();
+  return PXRB_OK;
 }
 
 int pxrb_particle_bcs_periodic(int64_t np, double* xp, double* yp, double* zp, double xmin,

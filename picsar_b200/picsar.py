@@ -72,10 +72,18 @@ def to_fortran(a, device="cuda", dtype=torch.float64):
 
 
 def is_fortran(t: torch.Tensor) -> bool:
+    """A 2-D or 3-D tensor in Fortran (column-major) layout."""
+    if t.dim() == 2:
+        return t.stride() == (1, t.shape[0])
     if t.dim() != 3:
         return False
     s0, s1, s2 = t.shape
     return t.stride() == (1, s0, s0 * s1)
+
+
+def grid2d_zeros(nx, nz, g, dtype=torch.float64, device="cuda"):
+    """A PICSAR x-z grid array (-g:n+g per axis) as a Fortran-ordered tensor."""
+    return fortran_zeros((nx + 1 + 2 * g, nz + 1 + 2 * g), dtype, device)
 
 
 def _ptr(t, name="array", grid=False, dtype=torch.float64):
@@ -951,6 +959,214 @@ def FD_weights(coeffs, norder, l_nodal):
         raise ValueError("coeffs: contiguous float64 array of norder/2 values")
     _lib.call("pxrb_fd_weights", c.ctypes.data, int(norder), int(bool(l_nodal)))
     return c
+
+
+# ---------------------------------------------------------------------------
+# 2D (x-z) routines (Forthon names and argument order)
+# ---------------------------------------------------------------------------
+def geteb2dxz_energy_conserving(np_, xp, yp, zp, ex, ey, ez, bx, by, bz, xmin, ymin, zmin, dx,
+                                dy, dz, nx, ny, nz, nxguard, nyguard, nzguard, nox, noy, noz,
+                                exg, eyg, ezg, bxg, byg, bzg, l4symtry, l_lower_order_in_v,
+                                lvect, field_gathe_algo, l_nodal=False):
+    """field_gathering_manager_2d.F90:61 (grids: 2-D x-z Fortran tensors;
+    l_nodal = module l_nodalgrid)."""
+    parts = [_ptr(a) for a in (xp, zp, ex, ey, ez, bx, by, bz)]
+    grids = [_ptr(a, grid=True) for a in (exg, eyg, ezg, bxg, byg, bzg)]
+    _lib.call("pxrb_geteb2dxz_energy_conserving", int(np_), parts[0],
+              None if yp is None else _ptr(yp), parts[1], *parts[2:], float(xmin),
+              float(ymin), float(zmin), float(dx), float(dy), float(dz), int(nx), int(ny),
+              int(nz), int(nxguard), int(nyguard), int(nzguard), int(nox), int(noy), int(noz),
+              *grids, int(bool(l4symtry)), int(bool(l_lower_order_in_v)), int(lvect),
+              int(field_gathe_algo), int(bool(l_nodal)), _stream())
+
+
+def depose_jxjyjz_2d(jx, jy, jz, np_, xp, yp, zp, uxp, uyp, uzp, gaminv, w, q, xmin, zmin, dt,
+                     dx, dz, nx, nz, nxguard, nzguard, nox, noz, lvect):
+    """current_deposition_manager_2d.F90:42 (2-D Esirkepov, accumulating)."""
+    _lib.call("pxrb_depose_jxjyjz_2d", *[_ptr(a, grid=True) for a in (jx, jy, jz)], int(np_),
+              _ptr(xp), None if yp is None else _ptr(yp), _ptr(zp),
+              *[_ptr(a) for a in (uxp, uyp, uzp, gaminv, w)], float(q), float(xmin),
+              float(zmin), float(dt), float(dx), float(dz), int(nx), int(nz), int(nxguard),
+              int(nzguard), int(nox), int(noz), int(lvect), _stream())
+
+
+def _b2(v):
+    a = np.ascontiguousarray(np.asarray(v, dtype=np.int64).reshape(2))
+    return a, a.ctypes.data
+
+
+def _yee2d(name, bounds, arrays, scalars):
+    keep, args = [], []
+    for v in bounds:
+        a, p = _b2(v); keep.append(a); args.append(p)
+    for arr, lo, hi in arrays:
+        a1, p1 = _b2(lo); a2, p2 = _b2(hi); keep += [a1, a2]
+        if tuple(arr.shape) != tuple(int(h - l + 1) for l, h in zip(a1, a2)):
+            raise ValueError(f"array shape {tuple(arr.shape)} does not match its bounds")
+        args += [_ptr(arr, grid=True), p1, p2]
+    _lib.call(name, *args, *[float(v) for v in scalars], _stream())
+
+
+def pxrpush_em2d_evec(xlo, xhi, ylo, yhi, zlo, zhi, ex, exlo, exhi, ey, eylo, eyhi, ez, ezlo,
+                      ezhi, bx, bxlo, bxhi, by, bylo, byhi, bz, bzlo, bzhi, jx, jxlo, jxhi, jy,
+                      jylo, jyhi, jz, jzlo, jzhi, mudt, dtsdx, dtsdy, dtsdz):
+    """yee.F90:216-310 (bounds of 2 values: x, z)."""
+    _yee2d("pxrb_push_em2d_evec", (xlo, xhi, ylo, yhi, zlo, zhi),
+           ((ex, exlo, exhi), (ey, eylo, eyhi), (ez, ezlo, ezhi), (bx, bxlo, bxhi),
+            (by, bylo, byhi), (bz, bzlo, bzhi), (jx, jxlo, jxhi), (jy, jylo, jyhi),
+            (jz, jzlo, jzhi)), (mudt, dtsdx, dtsdy, dtsdz))
+
+
+def pxrpush_em2d_bvec(xlo, xhi, ylo, yhi, zlo, zhi, ex, exlo, exhi, ey, eylo, eyhi, ez, ezlo,
+                      ezhi, bx, bxlo, bxhi, by, bylo, byhi, bz, bzlo, bzhi, dtsdx, dtsdy, dtsdz):
+    """yee.F90:912-994 (bounds of 2 values: x, z)."""
+    _yee2d("pxrb_push_em2d_bvec", (xlo, xhi, ylo, yhi, zlo, zhi),
+           ((ex, exlo, exhi), (ey, eylo, eyhi), (ez, ezlo, ezhi), (bx, bxlo, bxhi),
+            (by, bylo, byhi), (bz, bzlo, bzhi)), (dtsdx, dtsdy, dtsdz))
+
+
+def pxr_pushxz(np_, xp, zp, uxp, uzp, gaminv, dt):
+    """boris_2d.F90:42."""
+    _lib.call("pxrb_pushxz", int(np_), *[_ptr(a) for a in (xp, zp, uxp, uzp, gaminv)],
+              float(dt), _stream())
+
+
+class PicsarModule2D:
+    """Module variables and drivers of PICSAR's 2D (x-z) step loop on the
+    plain FP64 path (submain.F90, c_dim = 2): grids are x-z Fortran arrays
+    (-g:n+g) per axis; particles keep a y coordinate that is not pushed."""
+
+    def __init__(self, nx, nz, nguards=3, dx=1.0, dz=1.0, xmin=0.0, zmin=0.0, dtcoef=0.95,
+                 dt=None, nox=1, particle_pusher=0, clight=1.0, mu0=1.0, eps0=1.0,
+                 device="cuda"):
+        self.device = torch.device(device)
+        self.nx, self.nz = int(nx), int(nz)
+        self.ny = 0
+        self.nxguards = self.nzguards = int(nguards)
+        self.dx, self.dz = float(dx), float(dz)
+        self.xmin, self.zmin = float(xmin), float(zmin)
+        self.xmax, self.zmax = self.xmin + self.nx * self.dx, self.zmin + self.nz * self.dz
+        self.clight, self.mu0, self.eps0 = float(clight), float(mu0), float(eps0)
+        if dt is None:
+            # submain.F90:587
+            dt = dtcoef / (self.clight * math.sqrt(1.0 / self.dx ** 2 + 1.0 / self.dz ** 2))
+        self.dt = float(dt)
+        self.nox = self.noz = int(nox)
+        self.particle_pusher = int(particle_pusher)
+        self.l_nodalgrid = False
+        self.it = 0
+        g = self.nxguards
+        for name in ("ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz"):
+            setattr(self, name, grid2d_zeros(self.nx, self.nz, g, device=self.device))
+        self.species = []
+
+    def add_species(self, name, charge, mass, x, y, z, ux, uy, uz, w, pid=None):
+        dev, f = self.device, torch.float64
+        t = lambda a: torch.as_tensor(a, dtype=f).to(dev).contiguous()
+        sp = Species(name, float(charge), float(mass))
+        sp.part_x, sp.part_y, sp.part_z = t(x), t(y), t(z)
+        sp.part_ux, sp.part_uy, sp.part_uz = t(ux), t(uy), t(uz)
+        n = sp.part_x.numel()
+        sp.part_gaminv = torch.empty(n, dtype=f, device=dev)
+        pxr_set_gamma(n, sp.part_ux, sp.part_uy, sp.part_uz, sp.part_gaminv, clight=self.clight)
+        for c in ("ex", "ey", "ez", "bx", "by", "bz"):
+            setattr(sp, "part_" + c, torch.zeros(n, dtype=f, device=dev))
+        sp.pid_w = t(w)
+        sp.pid_id = t(pid) if pid is not None else torch.arange(n, dtype=f, device=dev)
+        self.species.append(sp)
+        return sp
+
+    def field_gathering_plus_particle_pusher(self):
+        """particle_pusher_manager_2d.F90:57-278: zero the particle fields,
+        gather (l_lower_order_in_v = .TRUE.), push u (Vay or Boris), push x, z."""
+        for sp in self.species:
+            if sp.np == 0:
+                continue
+            for c in ("ex", "ey", "ez", "bx", "by", "bz"):
+                getattr(sp, "part_" + c).zero_()
+            geteb2dxz_energy_conserving(
+                sp.np, sp.part_x, sp.part_y, sp.part_z, sp.part_ex, sp.part_ey, sp.part_ez,
+                sp.part_bx, sp.part_by, sp.part_bz, self.xmin, 0.0, self.zmin, self.dx, 1.0,
+                self.dz, self.nx, 0, self.nz, self.nxguards, 0, self.nzguards, self.nox,
+                self.nox, self.noz, self.ex, self.ey, self.ez, self.bx, self.by, self.bz, False,
+                True, 256, 0, l_nodal=self.l_nodalgrid)
+            fields = (sp.part_ex, sp.part_ey, sp.part_ez, sp.part_bx, sp.part_by, sp.part_bz)
+            if self.particle_pusher == 1:
+                pxr_ebcancelpush3d(sp.np, sp.part_ux, sp.part_uy, sp.part_uz, sp.part_gaminv,
+                                   *fields, sp.charge, sp.mass, self.dt, 0, clight=self.clight)
+            else:
+                pxr_boris_push_u_3d(sp.np, sp.part_ux, sp.part_uy, sp.part_uz, sp.part_gaminv,
+                                    *fields, sp.charge, sp.mass, self.dt, clight=self.clight)
+            pxr_pushxz(sp.np, sp.part_x, sp.part_z, sp.part_ux, sp.part_uz, sp.part_gaminv,
+                       self.dt)
+
+    def particle_bcs(self):
+        """Periodic wrap in x and z (particle_boundaries.F90, 2D branch)."""
+        for sp in self.species:
+            if sp.np:
+                _lib.call("pxrb_particle_bcs_periodic", sp.np, _ptr(sp.part_x),
+                          _ptr(sp.part_y), _ptr(sp.part_z), self.xmin, -math.inf, self.zmin,
+                          self.xmax, math.inf, self.zmax, _stream())
+
+    def pxrdepose_currents_on_grid_jxjyjz(self):
+        """J = 0, then the 2-D Esirkepov deposition of every species
+        (current_deposition_manager_2d.F90:334)."""
+        self.jx.zero_(); self.jy.zero_(); self.jz.zero_()
+        for sp in self.species:
+            if sp.np == 0 or not sp.ldodepos:
+                continue
+            depose_jxjyjz_2d(self.jx, self.jy, self.jz, sp.np, sp.part_x, sp.part_y, sp.part_z,
+                             sp.part_ux, sp.part_uy, sp.part_uz, sp.part_gaminv, sp.pid_w,
+                             sp.charge, self.xmin, self.zmin, self.dt, self.dx, self.dz, self.nx,
+                             self.nz, self.nxguards, self.nzguards, self.nox, self.noz, 256)
+
+    def _bc(self, arrs, fold):
+        name = "pxrb_summation_bcs_periodic" if fold else "pxrb_field_bc_periodic"
+        _lib.call(name, *[_ptr(a, grid=True) for a in arrs], self.nx, 0, self.nz, self.nxguards,
+                  0, self.nzguards, _stream())
+
+    def current_bcs(self):
+        self._bc((self.jx, self.jy, self.jz), True)
+
+    def efield_bcs(self):
+        self._bc((self.ex, self.ey, self.ez), False)
+
+    def bfield_bcs(self):
+        self._bc((self.bx, self.by, self.bz), False)
+
+    def _bounds(self):
+        g = self.nxguards
+        lo, hi = (-g, -g), (self.nx + g, self.nz + g)
+        rng = ((0, 0), (self.nx, self.nz))
+        return lo, hi, rng
+
+    def push_bfield(self):
+        """B half step (maxwell_solver_manager.F90:453-500, order 2)."""
+        lo, hi, (a, b) = self._bounds()
+        pxrpush_em2d_bvec(a, b, a, b, a, b, self.ex, lo, hi, self.ey, lo, hi, self.ez, lo, hi,
+                          self.bx, lo, hi, self.by, lo, hi, self.bz, lo, hi,
+                          0.5 * self.dt / self.dx, 0.0, 0.5 * self.dt / self.dz)
+
+    def push_efield(self):
+        """E full step (maxwell_solver_manager.F90:510-560, order 2)."""
+        lo, hi, (a, b) = self._bounds()
+        c2 = self.clight ** 2
+        pxrpush_em2d_evec(a, b, a, b, a, b, self.ex, lo, hi, self.ey, lo, hi, self.ez, lo, hi,
+                          self.bx, lo, hi, self.by, lo, hi, self.bz, lo, hi, self.jx, lo, hi,
+                          self.jy, lo, hi, self.jz, lo, hi, c2 * self.mu0 * self.dt,
+                          c2 * self.dt / self.dx, 0.0, c2 * self.dt / self.dz)
+
+    def step(self, nst=1):
+        """2D PIC loop (submain.F90, c_dim = 2, Yee solver)."""
+        for _ in range(nst):
+            self.field_gathering_plus_particle_pusher()
+            self.particle_bcs()
+            self.pxrdepose_currents_on_grid_jxjyjz()
+            self.current_bcs()
+            self.push_bfield(); self.bfield_bcs()
+            self.push_efield(); self.efield_bcs()
+            self.push_bfield(); self.bfield_bcs()
+            self.it += 1
 
 
 def _check_bounds(arr, lo, hi):

@@ -260,6 +260,93 @@ def test_yee_norder(norder, nodal):
         _eq(x, y, f"yee norder {norder} {c}")
 
 
+# ---------------------------------------------------------------------------
+# 2D (x-z) path
+N2 = (N[0], N[2])
+D2 = (D[0], D[2])
+
+
+def _grids2d(seed, amp=0.3, k=6):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(k):
+        a = O.zeros_grid2d(*N2, G)
+        a[...] = amp * rng.standard_normal(a.shape)
+        out.append(a)
+    return out
+
+
+def _ng2():
+    ng, ngp = R.ivec(G, G)
+    nv, nvp = R.ivec(N2[0] + 1, N2[1] + 1)
+    return (ng, ngp), (nv, nvp)
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("lower,nodal", [(True, False), (False, False), (True, True)])
+def test_gather_2d(order, lower, nodal):
+    p = _parts(900 + order)
+    g = _grids2d(901 + order)
+    (ng, ngp), (nv, nvp) = _ng2()
+    for which, comps in ((0, ("ex", "ey", "ez")), (1, ("bx", "by", "bz"))):
+        a, b = _copy(p), _copy(p)
+        gg = g[:3] if which == 0 else g[3:]
+        O.geteb2dxz(which, a["x"], a["z"], *[a[c] for c in comps], XMIN[0], XMIN[2], *D2, N2,
+                    G, order, *gg, lower, nodal)
+        name = ("pxr_gete2dxz" if which == 0 else "pxr_getb2dxz") + \
+            f"_energy_conserving_scalar_{order}_{order}"
+        R.call(name, R.i64(len(p["x"])), R.arr(b["x"]), R.arr(b["z"]),
+               *[R.arr(b[c]) for c in comps], R.f64(XMIN[0]), R.f64(XMIN[2]),
+               *[R.f64(v) for v in D2], *sum([[R.arr(x), ngp, nvp] for x in gg], []),
+               R.i64(int(lower)), R.i64(int(nodal)))
+        for c in comps:
+            _eq(a[c], b[c], f"2d gather {c} order {order}")
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_esirkepov_2d(order):
+    p = _parts(920 + order)
+    ja, jb = _grids2d(921, amp=0.0, k=3), _grids2d(921, amp=0.0, k=3)
+    (ng, ngp), (nv, nvp) = _ng2()
+    O.depose_jxjyjz_esirkepov2d(order, *ja, p["x"], p["z"], p["ux"], p["uy"], p["uz"],
+                                p["gaminv"], p["w"], Q, XMIN[0], XMIN[2], DT, *D2, N2, G)
+    R.call(f"pxr_depose_jxjyjz_esirkepov2d_{order}_{order}",
+           *sum([[R.arr(x), ngp, nvp] for x in jb], []), R.i64(len(p["x"])),
+           *[R.arr(p[c]) for c in ("x", "z", "ux", "uy", "uz", "gaminv", "w")], R.f64(Q),
+           R.f64(XMIN[0]), R.f64(XMIN[2]), R.f64(DT), *[R.f64(v) for v in D2], R.i64(64),
+           R.i64(1), R.i64(0), R.i64(0), R.i64(0))
+    for x, y, c in zip(ja, jb, ("jx", "jy", "jz")):
+        _eq(x, y, f"2d esirkepov {c} order {order}")
+
+
+def test_yee_2d_and_pushxz():
+    fa = _grids2d(940)
+    ja = _grids2d(941, k=3)
+    fb = [a.copy(order="F") for a in fa]
+    dtx, dtz = DT / D2[0], DT / D2[1]
+    O.push_em2d_bvec(*fa, N2, G, 0.5 * dtx, 0.5 * dtz)
+    O.push_em2d_evec(*fa, *ja, N2, G, DT, dtx, dtz)
+    lo, lop = R.ivec(-G, -G)
+    hi, hip = R.ivec(N2[0] + G, N2[1] + G)
+    b0, b0p = R.ivec(0, 0)
+    b1, b1p = R.ivec(*N2)
+    R.call("pxrpush_em2d_bvec", b0p, b1p, b0p, b1p, b0p, b1p,
+           *sum([[R.arr(f), lop, hip] for f in fb], []), R.f64(0.5 * dtx), R.f64(0.0),
+           R.f64(0.5 * dtz))
+    R.call("pxrpush_em2d_evec", b0p, b1p, b0p, b1p, b0p, b1p,
+           *sum([[R.arr(f), lop, hip] for f in fb + ja], []), R.f64(DT), R.f64(dtx),
+           R.f64(0.0), R.f64(dtz))
+    for x, y, c in zip(fa, fb, ("ex", "ey", "ez", "bx", "by", "bz")):
+        _eq(x, y, f"yee 2d {c}")
+    p = _parts(950)
+    a, b = _copy(p), _copy(p)
+    O.pushxz(a["x"], a["z"], a["ux"], a["uz"], a["gaminv"], DT)
+    R.call("pxr_pushxz", R.i64(len(p["x"])), R.arr(b["x"]), R.arr(b["z"]), R.arr(b["ux"]),
+           R.arr(b["uz"]), R.arr(b["gaminv"]), R.f64(DT))
+    _eq(a["x"], b["x"], "pushxz x")
+    _eq(a["z"], b["z"], "pushxz z")
+
+
 def test_comparison_detects_one_ulp():
     """The harness is not vacuous: a one-ulp change of dt on the oracle side
     changes the Boris result, and the equality check reports it."""
