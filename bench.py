@@ -840,30 +840,39 @@ def run_tiled_fp64(wl, args, ws, rank, cfg):
 
 def _plain_fp64_jobs(specs, steps=2):
     """Plain FP64 GPU path, one job at a time (PICSAR arrays, FP64 atomics):
-    per job 1 untimed step then `steps` timed steps (CUDA events).  Returns
-    (particle-steps/s over all jobs, {index: ms per step})."""
+    per job its setup (initial state, module, add_species; host wall clock
+    between device synchronisations), its first step and then `steps` more
+    steps (CUDA events).  Returns (particle-steps/s of the timed steps over
+    all jobs, {index: ms per step}, {index: seconds of setup and first step
+    beyond one step})."""
     import torch
     from picsar_b200.picsar import PicsarModule
-    per, tot_ps, tot_ms = {}, 0, 0.0
+    per, extra, tot_ps, tot_ms = {}, {}, 0, 0.0
     s = torch.cuda.current_stream()
     for i, sp in enumerate(specs):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         st = sp.initial_state(device="cuda")
         m = PicsarModule(*sp.n, nguards=3, nox=sp.order, particle_pusher=sp.pusher)
         m.add_species("electron", -1.0, 1.0, st.x, st.y, st.z, st.ux, st.uy, st.uz, st.w)
         del st
-        m.step(1)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(s)
-        m.step(steps)
-        b.record(s)
         torch.cuda.synchronize()
-        ms = a.elapsed_time(b)
+        setup_s = time.perf_counter() - t0
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(s)
+        m.step(1)
+        ev[1].record(s)
+        m.step(steps)
+        ev[2].record(s)
+        torch.cuda.synchronize()
+        ms = ev[1].elapsed_time(ev[2])
         per[i] = ms / steps
+        extra[i] = setup_s + max(0.0, ev[0].elapsed_time(ev[1]) - per[i]) * 1e-3
         tot_ps += sp.particles * steps
         tot_ms += ms
         del m
     torch.cuda.empty_cache()
-    return tot_ps / (tot_ms * 1e-3), per
+    return tot_ps / (tot_ms * 1e-3), per, extra
 
 
 def _tuned_configs(specs, precision="fp32"):
@@ -976,7 +985,7 @@ def run_ensemble(args):
     fp64 = None
     if not args.skip_fp64:
         sample = specs[::max(1, len(specs) // args.fp64_jobs)][:args.fp64_jobs]
-        rate64, _ = _plain_fp64_jobs(sample, steps=2)
+        rate64, _, _ = _plain_fp64_jobs(sample, steps=2)
         fp64 = {"value": rate64 * ws, "unit": "particle-steps/s", "jobs_sampled": len(sample),
                 "what": "plain FP64 GPU path, jobs launched one at a time (sampled jobs, "
                         "2 timed steps each after 1 untimed)"}
@@ -1024,7 +1033,8 @@ def run_serve(args):
     stream, each job's service time measured on the plain FP64 path."""
     import torch
     from picsar_b200.ensemble import ensemble_jobs
-    from picsar_b200.serve import Server, fifo_latencies, percentile, poisson_requests
+    from picsar_b200.serve import (Server, fifo_latencies, percentile, poisson_requests,
+                                   serve_fifo_plain)
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
     rates = [float(x) for x in args.rates.split(",")]
@@ -1034,10 +1044,16 @@ def run_serve(args):
     for o, c in configs.items():
         tune_info[str(o)]["acc"] = c.acc
     # warm-up: a few short jobs through the server (kernel attributes, pools)
+    # and the initial states of the stream's largest jobs (the generator's
+    # kernels for those sizes load on first use)
     warm = ensemble_jobs(count=6, seed=5, steps=3, cells=(16, 24))
     Server("fp32", configs=configs).run(poisson_requests(warm, 1e6), clock="wall")
-    _, per_ms = _plain_fp64_jobs(specs, steps=2)
-    service = {i: per_ms[i] * specs[i].steps / 1e3 for i in range(len(specs))}
+    for sp in sorted(specs, key=lambda x: -x.particles)[:4]:
+        sp.initial_state(device="cuda")
+    # per job the plain FP64 service time: setup and first step, then its
+    # remaining steps at the measured time per step
+    _, per_ms, extra_s = _plain_fp64_jobs(specs, steps=2)
+    service = {i: extra_s[i] + per_ms[i] * specs[i].steps / 1e3 for i in range(len(specs))}
     sweep = []
     clocks = ClockSampler(local)
     clocks.start()
@@ -1054,6 +1070,17 @@ def run_serve(args):
                                     "particle_steps_per_s":
                                         sum(sp.particles * sp.steps for sp in specs) / fifo_span}})
     clk = clocks.stop()
+    # the one-at-a-time FP64 stream actually served at one rate, against the
+    # model built from the separately measured service times
+    lam = args.fifo_rate
+    reqs = poisson_requests(specs, lam, seed=2000)
+    srep = serve_fifo_plain(reqs).summary()
+    fifo = fifo_latencies(reqs, service)
+    fl = list(fifo.values())
+    fifo_served = {"rate_jobs_per_s": lam, "served": srep,
+                   "model": {"p50_latency_s": percentile(fl, 50),
+                             "p99_latency_s": percentile(fl, 99)},
+                   "p50_served_over_model": srep["p50_latency_s"] / percentile(fl, 50)}
     if rank == 0:
         top = max(sweep, key=lambda x: x["particle_steps_per_s"])
         line = {
@@ -1068,6 +1095,7 @@ def run_serve(args):
                        "autotune_seconds": tune_s},
             "sweep": sweep, "clocks": clk,
             "fp64_service_s_total": sum(service.values()),
+            "fp64_fifo_served": fifo_served,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -1088,6 +1116,8 @@ def main():
     ap.add_argument("--fp64-jobs", type=int, default=24)
     ap.add_argument("--rates", default="10,20,50,100,200")
     ap.add_argument("--hbm-budget", type=float, default=150.0, help="GB")
+    ap.add_argument("--fifo-rate", type=float, default=50.0,
+                    help="rate (jobs/s) of the served one-at-a-time FP64 baseline")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--ctas-per-sm", type=int, default=2)

@@ -33,7 +33,7 @@ import torch
 
 from . import _lib
 from .init import thermal_plasma
-from .tiled import TiledConfig, TiledJob, TiledSim, _stream
+from .tiled import TiledConfig, TiledJob, TiledSim, _stream, h2d
 
 _lib.register({"pxrb_tiled_sort_batch": "p I I I i s", "pxrb_tiled_relayout": "p I I I i s"})
 
@@ -107,6 +107,19 @@ def job_bytes(spec: JobSpec, precision="fp32", config: TiledConfig | None = None
     return int(grid + parts + (1 << 16))
 
 
+_CAPTURE_STREAMS = {}
+
+
+def _capture_stream(dev):
+    """The stream graphs are captured on (one per device, from torch's
+    high-priority pool, so that it is not one of the low-priority pool
+    streams other code keeps for its own work)."""
+    s = _CAPTURE_STREAMS.get(dev.index)
+    if s is None:
+        s = _CAPTURE_STREAMS[dev.index] = torch.cuda.Stream(device=dev, priority=-1)
+    return s
+
+
 class _Group:
     """Jobs of one shape order: one particle-kernel launch and one batched
     sort per step / sort interval."""
@@ -152,14 +165,39 @@ class Ensemble:
         self.rebuild()
 
     # ----------------------------------------------------------------- setup
-    def _make_member(self, spec, state=None):
+    def _make_member(self, spec, state=None, diag_out=None):
+        """A job's simulation, loaded and sorted on the current stream.
+        diag_out: optional DEVICE float64[9] that receives the FP64
+        diagnostics (with the Gauss residual) of the loaded state, taken
+        before the sort so that no descriptor is read back."""
         sim = TiledSim(spec.n, order=spec.order, pusher=spec.pusher, precision=self.precision,
                        config=self.configs[spec.order], track_ids=self.track_ids,
                        device=self.device)
         st = state if state is not None else spec.initial_state(device=self.device)
-        sim.load_state(st)
+        sim.load_particles(st.x, st.y, st.z, st.ux, st.uy, st.uz, st.w, sort=False)
+        del st
+        if diag_out is not None:
+            diag_out.copy_(sim.diagnostics(gauss=True, to_host=False, pull=False))
+        sim.sort()
         self.launches += sim.launches
         return [spec, sim]
+
+    def prepare(self, spec, state=None, diag_out=None):
+        """Build a job's member on the current stream without adding it (see
+        join)."""
+        return self._make_member(spec, state, diag_out)
+
+    def join(self, members):
+        """Add prepared members (their preparation must be complete on, or
+        ordered before, the current stream) and repack on the device."""
+        self.members.extend(members)
+        self.rebuild(pull=False)
+
+    def leave(self, members):
+        """Retire members and repack on the device; the retired simulations
+        keep their state (and descriptors) for reading."""
+        self.remove(members)
+        self.rebuild(pull=False)
 
     def add(self, spec, state=None):
         """Admit one more job (the caller rebuilds before the next step)."""
@@ -173,9 +211,13 @@ class Ensemble:
         ids = {id(m) for m in members}
         self.members = [m for m in self.members if id(m) not in ids]
 
-    def rebuild(self):
+    def rebuild(self, pull=True):
         """Pack descriptors, group by order, build work lists and per-job
-        cell offsets for the current membership."""
+        cell offsets for the current membership.  pull=True packs the host
+        descriptors after reading each back from the device (one host
+        synchronisation per member); pull=False packs on the device by
+        copying each member's current device descriptor (no host
+        synchronisation: the serving loop's path)."""
         self.members.sort(key=lambda m: m[0].order)
         self._graph = None
         self._sort_graphs = {}
@@ -185,11 +227,16 @@ class Ensemble:
             self.groups = []
             return
         sz = C.sizeof(TiledJob)
-        host = bytearray(sz * nj)
-        for k, (sp, sim) in enumerate(self.members):
-            sim._pull_job()          # re-layouts may have exchanged its particle buffers
-            host[k * sz:(k + 1) * sz] = bytes(sim.job)
-        self.jobs_dev = torch.frombuffer(host, dtype=torch.uint8).to(self.device)
+        if pull:
+            host = bytearray(sz * nj)
+            for k, (sp, sim) in enumerate(self.members):
+                sim._pull_job()      # re-layouts may have exchanged its particle buffers
+                host[k * sz:(k + 1) * sz] = bytes(sim.job)
+            self.jobs_dev = torch.frombuffer(host, dtype=torch.uint8).to(self.device)
+        else:
+            # (a retired member keeps its old slot: its job_dev view holds
+            # the previous packed array)
+            self.jobs_dev = torch.cat([sim.job_dev for _, sim in self.members])
         # each member's device descriptor is its slot of the packed array, so
         # the member sees what the batched launches change there
         for k, (sp, sim) in enumerate(self.members):
@@ -214,7 +261,7 @@ class Ensemble:
             w = np.concatenate([np.stack([np.full(nt, jj, np.int32),
                                           np.arange(nt, dtype=np.int32)], 1)
                                 for _, jj, nt in items])
-            grp.work = torch.from_numpy(np.ascontiguousarray(w)).to(self.device)
+            grp.work = h2d(torch.from_numpy(np.ascontiguousarray(w)), self.device)
             grp.nwork = int(w.shape[0])
             grp.ctr = torch.zeros(1, dtype=torch.int32, device=self.device)
             self.groups.append(grp)
@@ -223,7 +270,7 @@ class Ensemble:
         for sp, sim in self.members:
             offs.append(offs[-1] + -(-sp.cells // 1024) * 1024)
         self.total_cells = offs[-1]
-        self.cell_off = torch.tensor(offs, dtype=torch.int64, device=self.device)
+        self.cell_off = h2d(torch.tensor(offs, dtype=torch.int64), self.device)
         self.particles_total = sum(sim.np for _, sim in self.members)
 
     # -------------------------------------------------------------- stepping
@@ -252,14 +299,20 @@ class Ensemble:
                   grp.count, self.prec, grp.max_tiles, grp.max_np, _stream())
 
     def _capture(self, fn):
-        # warm up once on a side stream (sets kernel attributes), then capture
-        side = torch.cuda.Stream(device=self.device)
-        side.wait_stream(torch.cuda.current_stream())
+        """fn's launches captured in a CUDA graph on a side stream.  fn has
+        run eagerly once before (kernel attributes are set), and nothing is
+        allocated inside it, so the capture needs no device synchronisation
+        (torch.cuda.graph would synchronise the device and empty the cache):
+        the device keeps running queued steps while the host captures, and a
+        replay orders after whatever precedes it on the replaying stream."""
+        side = _capture_stream(self.device)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.stream(side):
-            with torch.cuda.graph(g, stream=side, capture_error_mode="thread_local"):
+            g.capture_begin(capture_error_mode="thread_local")
+            try:
                 fn()
-        torch.cuda.current_stream().wait_stream(side)
+            finally:
+                g.capture_end()
         return g
 
     def _run(self, key, fn):

@@ -96,6 +96,18 @@ class TiledConfig:
     acc: int = 2                # FP32 engine current accumulator (see picsar_b200.h)
 
 
+def h2d_bytes(buf):
+    """Host bytes staged in pinned memory for a non-blocking copy to the
+    device (torch keeps the pinned block until the copy has run).  A blocking
+    copy from pageable memory would synchronise the stream it is issued on."""
+    return torch.frombuffer(bytearray(buf), dtype=torch.uint8).pin_memory()
+
+
+def h2d(t, device):
+    """A host tensor on the device without blocking the host (see h2d_bytes)."""
+    return t.pin_memory().to(device, non_blocking=True)
+
+
 def _stream():
     return torch.cuda.current_stream().cuda_stream
 
@@ -154,12 +166,14 @@ class TiledSim:
         self.cell_cnt = torch.zeros(self.ntiles * tile[0] * tile[1] * tile[2], dtype=torch.int32,
                                     device=dev)
         self.counters = torch.zeros(4, dtype=torch.int32, device=dev)
-        self.work = torch.stack([torch.zeros(self.ntiles, dtype=torch.int32),
-                                 torch.arange(self.ntiles, dtype=torch.int32)], 1).contiguous().to(dev)
+        # (built on the device: a blocking host copy would wait for the stream)
+        self.work = torch.zeros((self.ntiles, 2), dtype=torch.int32, device=dev)
+        self.work[:, 1] = torch.arange(self.ntiles, dtype=torch.int32, device=dev)
         self.ctr = torch.zeros(1, dtype=torch.int32, device=dev)
         ncell = nx * ny * nz
         self.total_cells = -(-ncell // 1024) * 1024
-        self.cell_off = torch.tensor([0, self.total_cells], dtype=torch.int64, device=dev)
+        self.cell_off = torch.zeros(2, dtype=torch.int64, device=dev)
+        self.cell_off[1] = self.total_cells
         self.diag_out = torch.zeros(9, dtype=torch.float64, device=dev)
         self.track_ids = track_ids
         self.np = 0
@@ -204,8 +218,16 @@ class TiledSim:
         return C.addressof(self.job)
 
     def _push_job(self):
-        buf = bytes(self.job)
-        self.job_dev.copy_(torch.frombuffer(bytearray(buf), dtype=torch.uint8))
+        """Copy the host descriptor to the device in stream order, without
+        blocking the host."""
+        self.job_dev.copy_(h2d_bytes(bytes(self.job)), non_blocking=True)
+
+    def set_job_bytes(self, raw):
+        """Replace the host descriptor by `raw` (a host uint8 tensor holding a
+        copy of the device descriptor)."""
+        if raw.numel() != C.sizeof(TiledJob):
+            raise ValueError("descriptor size mismatch")
+        C.memmove(C.addressof(self.job), raw.data_ptr(), C.sizeof(TiledJob))
 
     def _pull_job(self):
         """Refresh the host descriptor from the device (the sort swaps the
@@ -213,13 +235,15 @@ class TiledSim:
         raw = self.job_dev.cpu().numpy().tobytes()
         C.memmove(C.addressof(self.job), raw, len(raw))
 
-    def load_particles(self, x, y, z, ux, uy, uz, w, ids=None, ids_dense=None):
+    def load_particles(self, x, y, z, ux, uy, uz, w, ids=None, ids_dense=None, sort=True):
         """Load particles given as PICSAR arrays (absolute FP64 positions),
         device tensors or host arrays (pinned host tensors are uploaded
         without blocking the host).  ids (tracked ids only): the particles'
         identifiers, by default 0..N-1; ids_dense: True when ids is a
         permutation of 0..N-1 (then particles() restores the id order by a
-        scatter instead of a sort)."""
+        scatter instead of a sort).  sort=False leaves the particles unsorted
+        (the caller sorts before stepping); the host descriptor then still
+        points at the arrays the device uses."""
         dev = self.device
 
         def f64(a):
@@ -258,7 +282,8 @@ class TiledSim:
         _lib.call("pxrb_tiled_load_particles", self._jp(), x.data_ptr(), y.data_ptr(),
                   z.data_ptr(), ux.data_ptr(), uy.data_ptr(), uz.data_ptr(), w.data_ptr(),
                   _stream())
-        self.sort()
+        if sort:
+            self.sort()
 
     def load_state(self, st):
         """Load a picsar_b200.init.PlasmaState."""
@@ -359,13 +384,15 @@ class TiledSim:
             self.relayout()
 
     # ----------------------------------------------------------- diagnostics
-    def diagnostics(self, gauss=True, to_host=True):
+    def diagnostics(self, gauss=True, to_host=True, pull=True):
         """FP64 energies and (gauss=True) the Gauss-law residual of the current
-        state; to_host=False leaves the 9 values in self.diag_out (device)."""
+        state; to_host=False leaves the 9 values in self.diag_out (device).
+        pull=False: the host descriptor is known to be current (no sort or
+        re-layout since the load), so it is not read back from the device."""
         n_scr = _lib.query("pxrb_tiled_diag_scratch", self._jp())
         if getattr(self, "_scratch", None) is None or self._scratch.numel() < n_scr:
             self._scratch = torch.zeros(n_scr, dtype=torch.float64, device=self.device)
-        if gauss:
+        if gauss and pull:
             self._pull_job()     # rho deposition reads the current particle arrays
         _lib.call("pxrb_tiled_diagnostics", self._jp(),
                   self.rho.data_ptr() if gauss else None, self._scratch.data_ptr(),
@@ -429,6 +456,19 @@ class TiledSim:
                 out = {k: v[order] for k, v in out.items()}
                 out["id"] = cur[order]
         return out
+
+    def tensors(self):
+        """Every device tensor this simulation owns (for stream bookkeeping
+        when it was built on another stream than the one that steps it)."""
+        out = []
+        for v in vars(self).values():
+            if torch.is_tensor(v):
+                out.append(v)
+            elif isinstance(v, (list, tuple)):
+                out.extend(t for t in v if torch.is_tensor(t))
+            elif isinstance(v, dict):
+                out.extend(t for t in v.values() if torch.is_tensor(t))
+        return [t for t in out if t.is_cuda]
 
     def state_bytes(self):
         """Device bytes held by this simulation."""

@@ -79,3 +79,25 @@ def test_job_bytes_matches_allocation(cuda):
     t.load_state(spec.initial_state())
     pred = job_bytes(spec, "fp32")
     assert t.state_bytes() <= pred <= t.state_bytes() * 1.2 + (1 << 20)
+
+
+def test_fifo_plain_baseline_serves_every_job(cuda):
+    from picsar_b200.serve import serve_fifo_plain
+    specs = [JobSpec(n=(16, 16, 16), ppc=1, sigma=0.02, order=1, steps=3, seed=i)
+             for i in range(3)]
+    rep = serve_fifo_plain([Request(i, s, 0.0) for i, s in enumerate(specs)])
+    s = rep.summary()
+    assert s["jobs"] == 3
+    lat = [r.latency for r in rep.results]
+    assert all(v > 0 for v in lat) and lat == sorted(lat)      # one at a time, in order
+
+
+def test_wall_clock_server_runs_a_stream(cuda):
+    from picsar_b200.ensemble import ensemble_jobs
+    from picsar_b200.serve import poisson_requests
+    specs = ensemble_jobs(count=8, seed=3, steps_range=(3, 12), cells=(16, 24))
+    rep = Server("fp32").run(poisson_requests(specs, 200.0, seed=1), clock="wall")
+    s = rep.summary()
+    assert s["jobs"] == 8 and s["max_gauss_drift"] < 1e-4
+    assert all(r.finished >= r.admitted >= r.arrival - 1e-9 for r in rep.results)
+    assert rep.particle_steps == sum(sp.particles * sp.steps for sp in specs)
