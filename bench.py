@@ -334,7 +334,9 @@ def run_reference_jobs(args):
 
 
 # ---------------------------------------------------------------------------
-def run_ours(args):
+def run_ours(args, emit=True):
+    """The default arm on a fixed workload; prints the JSON line (emit) and
+    returns it (rank 0; None on the other ranks)."""
     import torch
     from picsar_b200.init import thermal_plasma
     from picsar_b200.tiled import TiledConfig, TiledSim
@@ -426,7 +428,7 @@ def run_ours(args):
     # the tiled engine in FP64 on the same workload (the same engine, 1e-12
     # of the oracle), with its roofline
     fp64_tiled = None
-    if not args.skip_fp64 and prec == 0:
+    if not args.skip_fp64 and not getattr(args, "skip_fp64_tiled", False) and prec == 0:
         fp64_tiled = run_tiled_fp64(wl, args, ws, rank, cfg)
 
     # FP32 mixed vs FP64 vs the oracle from one developed state: one-step
@@ -489,11 +491,14 @@ def run_ours(args):
             "deferred_fraction": deferred,
             "accuracy": accuracy,
         }
-        print(json.dumps(line), flush=True)
-    if ws > 1:
+        if ws == 1 and args.workload == "large" and not getattr(args, "skip_workloads", False):
+            line["workloads"] = _workload_legs(args)
+        if emit:
+            print(json.dumps(line), flush=True)
+    if ws > 1 and emit:
         import torch.distributed as dist
         dist.destroy_process_group()
-    return 0
+    return line if rank == 0 else None
 
 
 def _smem_roofline(wl, prec, cfg, N, kern_ms, clk):
@@ -934,25 +939,17 @@ def _ensemble_accuracy(specs, configs, steps):
             "gauss_residual_ratio_min": float(min(gr))}
 
 
-def run_ensemble(args):
-    """Batched ensemble of uneven jobs (256 periodic thermal plasmas, cells
-    per axis U{16..96}, ppc in {1,2,4,8,16}, order in {1,2,3}, u_th
-    log-uniform 0.001-0.05, 100 steps each) in one persistent kernel set
-    replayed from CUDA graphs; autotuned per order; compared with the plain
-    FP64 path run job by job."""
+def _ensemble_measure(specs, configs, steps, warmup, ws, fp64_jobs, accuracy=True):
+    """The batched ensemble of `specs`: `warmup` untimed steps, `steps` timed
+    steps (CUDA events, max over ranks), the particle kernels' roofline, the
+    energy drift over the timed steps and the plain FP64 path on a sample of
+    `fp64_jobs` jobs run one at a time.  Returns a dict."""
     import torch
-    from picsar_b200.ensemble import Ensemble, ensemble_jobs
-    ws, rank, local = _dist()
-    torch.cuda.set_device(local)
-    total_steps = args.steps + args.warmup
-    specs = ensemble_jobs(count=args.jobs, seed=2024 + rank, steps=total_steps)
-    configs, tune_info, tune_s = _tuned_configs(specs)
-    configs = _with_acc(configs, args.acc)
-    for o, c in configs.items():
-        tune_info[str(o)]["acc"] = c.acc
+    from picsar_b200.ensemble import Ensemble
+    local = torch.cuda.current_device()
     ens = Ensemble(specs, "fp32", configs)
     N = ens.particles_total
-    ens.step(args.warmup)
+    ens.step(warmup)
     # kinetic energy is summed per tile by the particle kernel: read it after a step
     d0 = ens.diagnostics()
     pk_ms, yee_ms = ens.profile_steps(2)
@@ -963,7 +960,7 @@ def run_ensemble(args):
     _barrier(ws)
     clocks.start()
     a.record(stream)
-    ens.step(args.steps)
+    ens.step(steps)
     b.record(stream)
     _barrier(ws)
     clk = clocks.stop()
@@ -971,7 +968,7 @@ def run_ensemble(args):
     launches = ens.launches - l0
     d1 = ens.diagnostics()
     drift = [(y["total"] - x["total"]) / x["total"] for x, y in zip(d0, d1)]
-    value = N * ws * args.steps / (ms * 1e-3)
+    value = N * ws * steps / (ms * 1e-3)
     peak, peak_kind = _peaks()
     alg = ens.algorithmic_bytes()
     achieved = alg / (pk_ms * 1e-3) / 1e9
@@ -979,44 +976,73 @@ def run_ensemble(args):
     slow = ens.slow_path_count()
     del ens
     torch.cuda.empty_cache()
-    accuracy = None
-    if not args.skip_accuracy:
-        accuracy = _ensemble_accuracy(specs[::8][:32], configs, total_steps)
+    acc = None
+    if accuracy:
+        acc = _ensemble_accuracy(specs[::8][:32], configs, steps + warmup)
     fp64 = None
-    if not args.skip_fp64:
-        sample = specs[::max(1, len(specs) // args.fp64_jobs)][:args.fp64_jobs]
+    if fp64_jobs > 0:
+        sample = specs[::max(1, len(specs) // fp64_jobs)][:fp64_jobs]
         rate64, _, _ = _plain_fp64_jobs(sample, steps=2)
         fp64 = {"value": rate64 * ws, "unit": "particle-steps/s", "jobs_sampled": len(sample),
                 "what": "plain FP64 GPU path, jobs launched one at a time (sampled jobs, "
                         "2 timed steps each after 1 untimed)"}
+    return {
+        "value": value, "unit": "particle-steps/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": ms / steps, "particles": N, "jobs": len(specs),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_tile_step (one launch per order group)",
+                     "kernel_ms": pk_ms, "yee_ms": yee_ms, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": alg},
+        "gpu_launches": launches, "clocks": clk, "fp64_plain": fp64,
+        "speedup_vs_fp64_plain": value / fp64["value"] if fp64 else None,
+        "energy_drift": {"median_abs": float(statistics.median(abs(x) for x in drift)),
+                         "max_abs": float(max(abs(x) for x in drift))},
+        "error_flags": int(sum(flags)), "slow_path_particle_steps": slow,
+        "accuracy": acc,
+    }
+
+
+ENSEMBLE_DESC = ("uneven periodic thermal-plasma jobs (cells/axis U{16..96}, ppc {1,2,4,8,16}, "
+                 "order {1,2,3}, u_th log-U[0.001,0.05]), one batched step per iteration "
+                 "replayed from CUDA graphs")
+
+
+def run_ensemble(args):
+    """Batched ensemble of uneven jobs (256 periodic thermal plasmas, cells
+    per axis U{16..96}, ppc in {1,2,4,8,16}, order in {1,2,3}, u_th
+    log-uniform 0.001-0.05, 100 steps each) in one persistent kernel set
+    replayed from CUDA graphs; autotuned per order; compared with the plain
+    FP64 path run job by job."""
+    import torch
+    from picsar_b200.ensemble import ensemble_jobs
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    specs = ensemble_jobs(count=args.jobs, seed=2024 + rank, steps=args.steps + args.warmup)
+    configs, tune_info, tune_s = _tuned_configs(specs)
+    configs = _with_acc(configs, args.acc)
+    for o, c in configs.items():
+        tune_info[str(o)]["acc"] = c.acc
+    r = _ensemble_measure(specs, configs, args.steps, args.warmup, ws,
+                          0 if args.skip_fp64 else args.fp64_jobs,
+                          accuracy=not args.skip_accuracy)
     if rank == 0:
         line = {
-            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "metric": "particle-steps/s", "value": r["value"], "unit": "particle-steps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"ensemble: {len(specs)} uneven periodic thermal-plasma jobs "
-                                   "(cells/axis U{16..96}, ppc {1,2,4,8,16}, order {1,2,3}, "
-                                   "u_th log-U[0.001,0.05]), one batched step per iteration "
-                                   "replayed from CUDA graphs",
-                       "particles_per_gpu": N, "jobs": len(specs),
+            "config": {"workload": f"ensemble: {len(specs)} {ENSEMBLE_DESC}",
+                       "particles_per_gpu": r["particles"], "jobs": len(specs),
                        "precision": "FP32 mixed (FP64 J flush and energy sums)",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": f"inputs larger than L2 (particle SoA {N * 32 / 1e9:.1f} GB), no flush",
+                       "l2": "inputs larger than L2 (particle SoA "
+                             f"{r['particles'] * 32 / 1e9:.1f} GB), no flush",
                        "autotuned": tune_info, "autotune_seconds": tune_s},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": "k_tile_step (one launch per order group)",
-                         "kernel_ms": pk_ms, "yee_ms": yee_ms, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": alg},
-            "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
-            "fp64_plain": fp64,
-            "fp64_tiled": fp64_tiled,
-            "speedup_vs_fp64_plain": value / fp64["value"] if fp64 else None,
-            "energy_drift": {"median_abs": float(statistics.median(abs(x) for x in drift)),
-                             "max_abs": float(max(abs(x) for x in drift))},
-            "error_flags": int(sum(flags)), "slow_path_particle_steps": slow,
-            "accuracy": accuracy,
+            "cpu_baseline": None, "e2e": None,
+            **{k: r[k] for k in ("roofline", "gpu_launches", "clocks", "fp64_plain",
+                                 "speedup_vs_fp64_plain", "energy_drift", "error_flags",
+                                 "slow_path_particle_steps", "accuracy")},
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -1025,24 +1051,17 @@ def run_ensemble(args):
     return 0
 
 
-def run_serve(args):
-    """Served stream: Poisson arrivals at each rate of --rates (jobs/s) of
-    jobs from the ensemble distribution with steps U{50..500}, admitted by
-    an HBM budget, continuously batched; p50/p99 latency and throughput,
-    against one-job-at-a-time plain FP64 execution (FIFO) of the same
-    stream, each job's service time measured on the plain FP64 path."""
+def _serve_measure(specs, configs, rates, hbm_budget_gb, fifo_rate):
+    """The served stream of `specs` at each Poisson rate (jobs/s, arrivals
+    seeded by the rate), continuously batched, against the one-at-a-time
+    plain FP64 FIFO model built from each job's measured service time, and
+    the FIFO stream actually served at `fifo_rate` (None: not served).
+    Returns a dict."""
     import torch
     from picsar_b200.ensemble import ensemble_jobs
     from picsar_b200.serve import (Server, fifo_latencies, percentile, poisson_requests,
                                    serve_fifo_plain)
-    ws, rank, local = _dist()
-    torch.cuda.set_device(local)
-    rates = [float(x) for x in args.rates.split(",")]
-    specs = ensemble_jobs(count=args.jobs, seed=77 + rank, steps_range=(50, 500))
-    configs, tune_info, tune_s = _tuned_configs(specs)
-    configs = _with_acc(configs, args.acc)
-    for o, c in configs.items():
-        tune_info[str(o)]["acc"] = c.acc
+    local = torch.cuda.current_device()
     # warm-up: a few short jobs through the server (kernel attributes, pools)
     # and the initial states of the stream's largest jobs (the generator's
     # kernels for those sizes load on first use)
@@ -1054,12 +1073,13 @@ def run_serve(args):
     # remaining steps at the measured time per step
     _, per_ms, extra_s = _plain_fp64_jobs(specs, steps=2)
     service = {i: extra_s[i] + per_ms[i] * specs[i].steps / 1e3 for i in range(len(specs))}
+    work = sum(sp.particles * sp.steps for sp in specs)
     sweep = []
     clocks = ClockSampler(local)
     clocks.start()
-    for k, lam in enumerate(rates):
-        reqs = poisson_requests(specs, lam, seed=1000 + k)
-        rep = Server("fp32", hbm_budget=int(args.hbm_budget * 1e9), configs=configs).run(reqs)
+    for lam in rates:
+        reqs = poisson_requests(specs, lam, seed=1000 + int(round(lam)))
+        rep = Server("fp32", hbm_budget=int(hbm_budget_gb * 1e9), configs=configs).run(reqs)
         s = rep.summary()
         fifo = fifo_latencies(reqs, service)
         fl = list(fifo.values())
@@ -1067,41 +1087,128 @@ def run_serve(args):
         sweep.append({"rate_jobs_per_s": lam, **s,
                       "fp64_fifo": {"p50_latency_s": percentile(fl, 50),
                                     "p99_latency_s": percentile(fl, 99),
-                                    "particle_steps_per_s":
-                                        sum(sp.particles * sp.steps for sp in specs) / fifo_span}})
+                                    "particle_steps_per_s": work / fifo_span}})
     clk = clocks.stop()
-    # the one-at-a-time FP64 stream actually served at one rate, against the
-    # model built from the separately measured service times
-    lam = args.fifo_rate
-    reqs = poisson_requests(specs, lam, seed=2000)
-    srep = serve_fifo_plain(reqs).summary()
-    fifo = fifo_latencies(reqs, service)
-    fl = list(fifo.values())
-    fifo_served = {"rate_jobs_per_s": lam, "served": srep,
-                   "model": {"p50_latency_s": percentile(fl, 50),
-                             "p99_latency_s": percentile(fl, 99)},
-                   "p50_served_over_model": srep["p50_latency_s"] / percentile(fl, 50)}
+    fifo_served = None
+    if fifo_rate:
+        # the one-at-a-time FP64 stream actually served at one rate, against
+        # the model built from the separately measured service times
+        reqs = poisson_requests(specs, fifo_rate, seed=2000)
+        srep = serve_fifo_plain(reqs).summary()
+        fifo = fifo_latencies(reqs, service)
+        fl = list(fifo.values())
+        fifo_served = {"rate_jobs_per_s": fifo_rate, "served": srep,
+                       "model": {"p50_latency_s": percentile(fl, 50),
+                                 "p99_latency_s": percentile(fl, 99)},
+                       "p50_served_over_model": srep["p50_latency_s"] / percentile(fl, 50)}
+    return {"sweep": sweep, "clocks": clk, "fp64_service_s_total": sum(service.values()),
+            "fp64_fifo_served": fifo_served}
+
+
+SERVE_DESC = ("jobs per rate from the ensemble distribution, steps U{50..500}, Poisson "
+              "arrivals, continuous batching")
+
+
+def run_serve(args):
+    """Served stream: Poisson arrivals at each rate of --rates (jobs/s) of
+    jobs from the ensemble distribution with steps U{50..500}, admitted by
+    an HBM budget, continuously batched; p50/p99 latency and throughput,
+    against one-job-at-a-time plain FP64 execution (FIFO) of the same
+    stream, each job's service time measured on the plain FP64 path."""
+    import torch
+    from picsar_b200.ensemble import ensemble_jobs
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    rates = [float(x) for x in args.rates.split(",")]
+    specs = ensemble_jobs(count=args.jobs, seed=77 + rank, steps_range=(50, 500))
+    configs, tune_info, tune_s = _tuned_configs(specs)
+    configs = _with_acc(configs, args.acc)
+    for o, c in configs.items():
+        tune_info[str(o)]["acc"] = c.acc
+    r = _serve_measure(specs, configs, rates, args.hbm_budget, args.fifo_rate)
     if rank == 0:
-        top = max(sweep, key=lambda x: x["particle_steps_per_s"])
+        top = max(r["sweep"], key=lambda x: x["particle_steps_per_s"])
         line = {
             "metric": "particle-steps/s", "value": top["particle_steps_per_s"] * ws,
             "unit": "particle-steps/s", "n_gpus": ws, "steps": None, "warmup": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"served stream: {len(specs)} jobs per rate from the ensemble "
-                                   "distribution, steps U{50..500}, Poisson arrivals, HBM budget "
-                                   f"{args.hbm_budget:g} GB, continuous batching",
+            "config": {"workload": f"served stream: {len(specs)} {SERVE_DESC}, HBM budget "
+                                   f"{args.hbm_budget:g} GB",
                        "rates_jobs_per_s": rates, "autotuned": tune_info,
                        "autotune_seconds": tune_s},
-            "sweep": sweep, "clocks": clk,
-            "fp64_service_s_total": sum(service.values()),
-            "fp64_fifo_served": fifo_served,
+            **r,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def _workload_legs(args):
+    """Compact single-GPU measurements of the other workloads, reported in
+    the default line: the ensemble (256 jobs, 20 timed steps, plain FP64 on
+    24 sampled jobs), the served stream (48 jobs at 50 and 200 jobs/s, the
+    FIFO FP64 stream served at 50 jobs/s) and the uneven-density workload
+    (20 timed steps, plain FP64 on the same state).  A leg that raises
+    reports its error instead of a number."""
+    import copy
+    import torch
+    from picsar_b200.ensemble import ensemble_jobs
+    out = {}
+
+    def leg(name, fn):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:                      # report, keep the headline
+            out[name] = {"error": repr(e)[:400]}
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        out[name]["leg_seconds"] = time.perf_counter() - t0
+
+    state = {}
+
+    def ensemble():
+        specs = ensemble_jobs(count=256, seed=2024, steps=23)
+        configs, tune_info, tune_s = _tuned_configs(specs)
+        configs = _with_acc(configs, args.acc)
+        state["configs"] = configs
+        r = _ensemble_measure(specs, configs, 20, 3, 1, 24, accuracy=False)
+        r["workload"] = f"ensemble: 256 {ENSEMBLE_DESC}"
+        r["autotune_seconds"] = tune_s
+        return r
+
+    def serve():
+        specs = ensemble_jobs(count=48, seed=77, steps_range=(50, 500))
+        configs = state.get("configs")
+        if configs is None:
+            configs = _with_acc(_tuned_configs(specs)[0], args.acc)
+        r = _serve_measure(specs, configs, [50.0, 200.0], args.hbm_budget, 50.0)
+        r["workload"] = f"served stream: 48 {SERVE_DESC}, HBM budget {args.hbm_budget:g} GB"
+        return r
+
+    def uneven():
+        a = copy.copy(args)
+        a.workload, a.steps, a.warmup = "uneven", 20, 3
+        a.skip_e2e = a.skip_cpu = a.skip_accuracy = a.skip_fp64_tiled = True
+        a.skip_workloads = True
+        r = run_ours(a, emit=False)
+        keep = ("value", "unit", "ms_per_step", "steps", "warmup", "roofline", "fp64_plain",
+                "gpu_launches", "clocks", "slow_path_particle_steps", "deferred_fraction")
+        d = {k: r[k] for k in keep}
+        d["workload"] = r["config"]["workload"]
+        d["tuning"] = r["config"]["tuning"]
+        d["tile_occupancy"] = r["config"]["tile_occupancy"]
+        d["speedup_vs_fp64_plain"] = (r["value"] / r["fp64_plain"]["value"]
+                                      if r.get("fp64_plain") else None)
+        return d
+
+    leg("ensemble", ensemble)
+    leg("serve", serve)
+    leg("uneven", uneven)
+    return out
 
 
 def main():
@@ -1133,6 +1240,9 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--skip-workloads", action="store_true",
+                    help="leave out the compact ensemble / serve / uneven legs of the "
+                         "default line")
     ap.add_argument("--accuracy-steps", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
@@ -1147,7 +1257,8 @@ def main():
         return run_ensemble(args)
     if args.workload == "serve":
         return run_serve(args)
-    return run_ours(args)
+    run_ours(args)
+    return 0
 
 
 if __name__ == "__main__":
