@@ -745,32 +745,67 @@ def run_e2e(st, wl, args, ws, cfg):
     m = PicsarModule(*wl["n"], nguards=3, nox=wl["order"], particle_pusher=wl["pusher"],
                      engine="tiled", precision=args.precision, tiled_config=cfg)
     stream = torch.cuda.current_stream()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     _barrier(ws)
     w0 = time.perf_counter()
-    a.record(stream)
+    ev[0].record(stream)
     m.add_species("electron", -1.0, 1.0, host["x"], host["y"], host["z"], host["ux"],
                   host["uy"], host["uz"], host["w"])
+    ev[1].record(stream)
     for s_ in range(args.steps):
         m.step(1)
         diag_host[s_].copy_(m.diagnostics(gauss=False, to_host=False), non_blocking=True)
+    ev[2].record(stream)
     sp = m.species[0]
     for c in out_cols:
         out_host[c].copy_(getattr(sp, c), non_blocking=True)
-    b.record(stream)
+    ev[3].record(stream)
     _barrier(ws)
     wall = time.perf_counter() - w0
-    ms = _max_over_ranks(a.elapsed_time(b), ws)
+    ms = _max_over_ranks(ev[0].elapsed_time(ev[3]), ws)
+    phases = {"add_species_ms": ev[0].elapsed_time(ev[1]),
+              "steps_ms": ev[1].elapsed_time(ev[2]),
+              "download_ms": ev[2].elapsed_time(ev[3])}
     del m
     torch.cuda.empty_cache()
     h2d = 7 * 8 * N
     d2h = len(out_cols) * 8 * N + args.steps * 9 * 8
-    return {"value": N * ws * args.steps / (ms * 1e-3), "unit": "particle-steps/s",
+    # the host link: pinned copies of 1 GiB each way; the end-to-end bound is
+    # the steps plus both transfers at that bandwidth, with nothing overlapped
+    bw = _pcie_gbs()
+    bound_s = phases["steps_ms"] * 1e-3 + h2d / (bw["h2d_gbs"] * 1e9) + d2h / (bw["d2h_gbs"] * 1e9)
+    bound = N * ws * args.steps / bound_s
+    value = N * ws * args.steps / (ms * 1e-3)
+    return {"value": value, "unit": "particle-steps/s",
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-            "ms": ms, "wall_s": wall,
+            "ms": ms, "wall_s": wall, "phases": phases, "host_link": bw,
+            "transfer_bound_value": bound, "frac_of_transfer_bound": value / bound,
             "what": "job through PicsarModule(engine='tiled'): PICSAR FP64 particle arrays "
                     "from pinned host memory (add_species), every step with its FP64 energies "
                     "copied to the host, final x, y, z, u, gamma^-1 arrays copied to the host"}
+
+
+def _pcie_gbs(nbytes=1 << 30, reps=3):
+    """Pinned host <-> device copy bandwidth (GB/s) of this GPU's host link,
+    best of `reps` copies of `nbytes` each way (CUDA events)."""
+    import torch
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s = torch.cuda.current_stream()
+    out = {}
+    for name, dst, src in (("h2d_gbs", d, h), ("d2h_gbs", h, d)):
+        best = None
+        for _ in range(reps + 1):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            dst.copy_(src, non_blocking=True)
+            b.record(s)
+            b.synchronize()
+            t = a.elapsed_time(b)
+            best = t if best is None else min(best, t)
+        out[name] = nbytes / (best * 1e-3) / 1e9
+    del h, d
+    return out
 
 
 def run_plain_fp64(wl, args, ws, rank):

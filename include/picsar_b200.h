@@ -465,6 +465,17 @@ int pxrb_tiled_load_particles(const pxrb_tiled_job* job_host, const double* x,
 int pxrb_tiled_store_particles(const pxrb_tiled_job* job_host, double* x, double* y,
                                double* z, double* ux, double* uy, double* uz,
                                double* gaminv, double* w, void* stream);
+/* The same conversion to PICSAR's arrays in the order the particles were
+ * added: particle i of the engine goes to row pid[i] of every output (the
+ * tracked ids must be a permutation of 0..np-1; rows outside [0, np) are
+ * skipped).  The particle pointers and ids are read from the DEVICE
+ * descriptor job_dev, so no read-back is needed after sorts; np and prec
+ * (0 FP32, 1 FP64) are the job's.  Nothing is written when the descriptor
+ * tracks no ids.  One pass, in place of a conversion plus one scatter per
+ * column. */
+int pxrb_tiled_store_particles_by_id(const pxrb_tiled_job* job_dev, int64_t np, int32_t prec,
+                                     double* x, double* y, double* z, double* ux, double* uy,
+                                     double* uz, double* gaminv, double* w, void* stream);
 int pxrb_tiled_field_import(const pxrb_tiled_job* job_host, int32_t which, const double* src,
                             int64_t nguard_src, void* stream);
 int pxrb_tiled_field_export(const pxrb_tiled_job* job_host, int32_t which, double* dst,

@@ -577,6 +577,35 @@ __global__ void k_store_particles(Job J, double* x, double* y, double* z, double
   }
 }
 
+// Engine -> PICSAR arrays in id order: particle p goes to row pid[p].  The
+// descriptor is read from device memory (one copy per block in shared memory).
+template <typename R>
+__global__ void k_store_particles_by_id(const Job* __restrict__ jd, i64 np, double* x,
+                                        double* y, double* z, double* ux, double* uy,
+                                        double* uz, double* gaminv, double* w) {
+  __shared__ Job J;
+  if (threadIdx.x == 0) J = *jd;
+  __syncthreads();
+  if (!J.pid) return;
+  const i64 n = J.np < np ? J.np : np;
+  for (i64 p = blockIdx.x * (i64)blockDim.x + threadIdx.x; p < n;
+       p += (i64)gridDim.x * blockDim.x) {
+    const i64 d = J.pid[p];
+    if (d < 0 || d >= np) continue;
+    int i, j, k;
+    unpack_cell(J.cell[p], i, j, k);
+    if (x) x[d] = J.xmin + ((double)i + (double)((const R*)J.ox)[p]) * J.dx;
+    if (y) y[d] = J.ymin + ((double)j + (double)((const R*)J.oy)[p]) * J.dy;
+    if (z) z[d] = J.zmin + ((double)k + (double)((const R*)J.oz)[p]) * J.dz;
+    const double a = ((const R*)J.ux)[p], b = ((const R*)J.uy)[p], c = ((const R*)J.uz)[p];
+    if (ux) ux[d] = a;
+    if (uy) uy[d] = b;
+    if (uz) uz[d] = c;
+    if (gaminv) gaminv[d] = 1.0 / sqrt(1.0 + (a * a + b * b + c * c) / (J.clight * J.clight));
+    if (w) w[d] = ((const R*)J.w)[p];
+  }
+}
+
 // Fortran guarded FP64 grid (ng guards) <-> engine.  dir 0: import, 1: export.
 template <typename R>
 __global__ void k_field_xfer(Job J, int which, double* f, int ng, int dir) {
@@ -934,6 +963,23 @@ int pxrb_tiled_store_particles(const pxrb_tiled_job* job_host, double* x, double
     k_store_particles<float><<<gs_blocks(J.np, 256), 256, 0, s>>>(J, x, y, z, ux, uy, uz, gaminv, w);
   else
     k_store_particles<double><<<gs_blocks(J.np, 256), 256, 0, s>>>(J, x, y, z, ux, uy, uz, gaminv, w);
+  PXRB_CHECK_LAUNCH();
+  return PXRB_OK;
+}
+
+int pxrb_tiled_store_particles_by_id(const pxrb_tiled_job* job_dev, int64_t np, int32_t prec,
+                                     double* x, double* y, double* z, double* ux, double* uy,
+                                     double* uz, double* gaminv, double* w, void* stream) {
+  if (!job_dev || np < 0) return PXRB_EINVAL;
+  if (prec < 0 || prec > 1) return PXRB_EUNSUPPORTED;
+  if (np == 0) return PXRB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (prec == 0)
+    k_store_particles_by_id<float><<<gs_blocks(np, 256), 256, 0, s>>>(job_dev, np, x, y, z, ux,
+                                                                      uy, uz, gaminv, w);
+  else
+    k_store_particles_by_id<double><<<gs_blocks(np, 256), 256, 0, s>>>(job_dev, np, x, y, z, ux,
+                                                                       uy, uz, gaminv, w);
   PXRB_CHECK_LAUNCH();
   return PXRB_OK;
 }

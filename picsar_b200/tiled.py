@@ -54,6 +54,7 @@ _lib.register({
     "pxrb_tiled_relayout": "p I I I i s",
     "pxrb_tiled_load_particles": "p p p p p p p p s",
     "pxrb_tiled_store_particles": "p p p p p p p p p s",
+    "pxrb_tiled_store_particles_by_id": "p i I p p p p p p p p s",
     "pxrb_tiled_field_import": "p I p i s",
     "pxrb_tiled_field_export": "p I p i s",
     "pxrb_tiled_diagnostics": "p p p i p s",
@@ -433,28 +434,27 @@ class TiledSim:
 
     def particles(self):
         """PICSAR-style FP64 particle arrays (sorted by id when ids are tracked)."""
-        self._pull_job()
         N, dev = self.np, self.device
         out = {c: torch.empty(N, dtype=torch.float64, device=dev)
                for c in ("x", "y", "z", "ux", "uy", "uz", "gaminv", "w")}
+        if self.track_ids and getattr(self, "_ids_dense", False):
+            # ids are the positions of the id order: one pass writes every
+            # column in that order, reading the current device descriptor
+            _lib.call("pxrb_tiled_store_particles_by_id", self.job_dev.data_ptr(), N, self.prec,
+                      *[out[c].data_ptr() for c in ("x", "y", "z", "ux", "uy", "uz", "gaminv",
+                                                    "w")], _stream())
+            out["id"] = torch.arange(N, dtype=torch.int32, device=dev)
+            return out
+        self._pull_job()
         _lib.call("pxrb_tiled_store_particles", self._jp(),
                   *[out[c].data_ptr() for c in ("x", "y", "z", "ux", "uy", "uz", "gaminv", "w")],
                   _stream())
         if self.track_ids and self.job.pid:
             C_ptr = self.job.pid
             cur = self.pid if self.pid.data_ptr() == C_ptr else self.pid_b
-            if getattr(self, "_ids_dense", False):
-                # ids are the positions of the id order: one scatter per array
-                idx = cur.long()
-                res = {}
-                for k, v in out.items():
-                    res[k] = torch.empty_like(v).index_copy_(0, idx, v)
-                res["id"] = torch.arange(N, dtype=torch.int32, device=dev)
-                out = res
-            else:
-                order = torch.argsort(cur.long())
-                out = {k: v[order] for k, v in out.items()}
-                out["id"] = cur[order]
+            order = torch.argsort(cur.long())
+            out = {k: v[order] for k, v in out.items()}
+            out["id"] = cur[order]
         return out
 
     def tensors(self):
