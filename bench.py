@@ -347,13 +347,13 @@ def run_ours(args, emit=True):
     prec = 0 if args.precision == "fp32" else 1
     cfg = TiledConfig(tile=wl["tile"], sort_interval=wl["sort_interval"], drift=1,
                       threads=args.threads, ctas_per_sm=args.ctas_per_sm, acc=args.acc,
-                      relayout_interval=args.relayout)
+                      relayout_interval=args.relayout, select_lanes=bool(args.select_lanes))
     tuned = None
     if wl.get("autotune"):
         from picsar_b200 import autotune
         r = autotune.tune(wl["order"], args.precision, ppc=wl["ppc"], sigma=wl["sigma"],
                           u_drift=wl.get("u_drift", 0.0),
-                          pusher=wl["pusher"])
+                          pusher=wl["pusher"], acc=args.acc)
         cfg = _with_acc({0: r.config}, args.acc)[0]
         tuned = {"proxy_rate": r.rate, "cached": r.cached}
     st = _initial_state(wl, 1234 + rank)
@@ -466,10 +466,11 @@ def run_ours(args, emit=True):
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "inputs larger than L2 (particle SoA "
                              f"{N * 32 / 1e9:.1f} GB per GPU), no flush",
-                       "tuning": {"tile": list(wl["tile"]), "drift": cfg.drift,
+                       "tuning": {"tile": list(cfg.tile), "drift": cfg.drift,
                                   "threads": cfg.threads, "ctas_per_sm": cfg.ctas_per_sm,
                                   "sort_interval": cfg.sort_interval,
                                   "relayout_interval": cfg.relayout_interval, "acc": cfg.acc,
+                                  "select_lanes": cfg.select_lanes,
                                   "autotuned": tuned},
                        "tile_occupancy": occupancy},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -642,7 +643,8 @@ def run_accuracy(wl, args, pusher, cfg, with_oracle=True):
     from picsar_b200.tiled import SUPPORTED_SHAPES_FP64, TiledConfig
     t0 = time.perf_counter()
     cfg = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval, drift=cfg.drift,
-                      threads=cfg.threads, acc=cfg.acc, relayout_interval=cfg.relayout_interval)
+                      threads=cfg.threads, acc=cfg.acc, relayout_interval=cfg.relayout_interval,
+                      select_lanes=cfg.select_lanes)
     cfg64 = cfg
     if (cfg.tile[0], cfg.drift) not in SUPPORTED_SHAPES_FP64:
         cfg64 = TiledConfig(tile=cfg.tile, sort_interval=cfg.sort_interval,
@@ -915,29 +917,32 @@ def _plain_fp64_jobs(specs, steps=2):
     return tot_ps / (tot_ms * 1e-3), per, extra
 
 
-def _tuned_configs(specs, precision="fp32"):
+def _tuned_configs(specs, precision="fp32", acc=2):
     from picsar_b200 import autotune
     t0 = time.perf_counter()
-    tuned = autotune.tune_ensemble(specs, precision)
+    tuned = autotune.tune_ensemble(specs, precision, acc=acc)
     dt = time.perf_counter() - t0
     info = {str(o): {"tile": r.config.tile[0], "drift": r.config.drift,
                      "threads": r.config.threads, "sort_interval": r.config.sort_interval,
                      "relayout_interval": r.config.relayout_interval,
+                     "select_lanes": r.config.select_lanes,
                      "proxy_rate": r.rate, "ppc": r.ppc, "sigma": r.sigma, "cached": r.cached}
             for o, r in tuned.items()}
     return {o: r.config for o, r in tuned.items()}, info, dt
 
 
 def _with_acc(configs, acc):
-    """Tuned configs with the requested FP32 accumulator mode (the tuner
-    times mode 2; mode 1 is compiled for 8^3 tiles with margin 1 only)."""
-    from picsar_b200.tiled import SUPPORTED_ACC, TiledConfig
+    """Configs with the requested FP32 accumulator mode where their shape
+    has it compiled (autotune.acc_for)."""
+    from picsar_b200.autotune import acc_for
+    from picsar_b200.tiled import TiledConfig
     out = {}
     for o, c in configs.items():
-        a = acc if acc in SUPPORTED_ACC.get((c.tile[0], c.drift), (2,)) else 2
+        a = acc_for(c.tile[0], c.drift, acc)
         out[o] = TiledConfig(tile=c.tile, drift=c.drift, threads=c.threads,
                              ctas_per_sm=c.ctas_per_sm, sort_interval=c.sort_interval, acc=a,
-                             relayout_interval=c.relayout_interval)
+                             relayout_interval=c.relayout_interval,
+                             select_lanes=c.select_lanes)
     return out
 
 
@@ -1054,7 +1059,7 @@ def run_ensemble(args):
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
     specs = ensemble_jobs(count=args.jobs, seed=2024 + rank, steps=args.steps + args.warmup)
-    configs, tune_info, tune_s = _tuned_configs(specs)
+    configs, tune_info, tune_s = _tuned_configs(specs, acc=args.acc)
     configs = _with_acc(configs, args.acc)
     for o, c in configs.items():
         tune_info[str(o)]["acc"] = c.acc
@@ -1156,7 +1161,7 @@ def run_serve(args):
     torch.cuda.set_device(local)
     rates = [float(x) for x in args.rates.split(",")]
     specs = ensemble_jobs(count=args.jobs, seed=77 + rank, steps_range=(50, 500))
-    configs, tune_info, tune_s = _tuned_configs(specs)
+    configs, tune_info, tune_s = _tuned_configs(specs, acc=args.acc)
     configs = _with_acc(configs, args.acc)
     for o, c in configs.items():
         tune_info[str(o)]["acc"] = c.acc
@@ -1207,7 +1212,7 @@ def _workload_legs(args):
 
     def ensemble():
         specs = ensemble_jobs(count=256, seed=2024, steps=23)
-        configs, tune_info, tune_s = _tuned_configs(specs)
+        configs, tune_info, tune_s = _tuned_configs(specs, acc=args.acc)
         configs = _with_acc(configs, args.acc)
         state["configs"] = configs
         r = _ensemble_measure(specs, configs, 20, 3, 1, 24, accuracy=False)
@@ -1219,7 +1224,7 @@ def _workload_legs(args):
         specs = ensemble_jobs(count=48, seed=77, steps_range=(50, 500))
         configs = state.get("configs")
         if configs is None:
-            configs = _with_acc(_tuned_configs(specs)[0], args.acc)
+            configs = _with_acc(_tuned_configs(specs, acc=args.acc)[0], args.acc)
         r = _serve_measure(specs, configs, [50.0, 200.0], args.hbm_budget, 50.0)
         r["workload"] = f"served stream: 48 {SERVE_DESC}, HBM budget {args.hbm_budget:g} GB"
         return r
@@ -1269,6 +1274,9 @@ def main():
                     help="FP32 current accumulator: 1 int32 fixed point (default: energy drift "
                          "and Gauss residual within 1e-3 of FP64's, one-step field error "
                          "~1e-4), 2 two-word 64-bit fixed point (~1e-5, slower), 0 FP32")
+    ap.add_argument("--select-lanes", type=int, default=1, choices=[0, 1],
+                    help="FP32 particle kernel: lanes of distinct bank classes per warp with a "
+                         "second pass for the others (1) or one pass (0), fixed workloads")
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--skip-e2e", action="store_true")

@@ -357,6 +357,12 @@ typedef struct pxrb_tiled_job {
                                                particles per window cell, valid);
                                                written by each particle step,
                                                invalidated by the sort */
+  int32_t select_lanes;                     /* FP32 engine: 1 = each warp takes lanes of
+                                               distinct bank classes and defers the
+                                               others to a second, class-bucketed pass;
+                                               0 = one pass (faster when many particles
+                                               change cell per step) */
+  int32_t reserved;                         /* 0 */
 } pxrb_tiled_job;
 
 /* Tile shapes: cubic tiles of edge tx = ty = tz = `tile` in {4, 8} with window

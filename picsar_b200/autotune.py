@@ -10,7 +10,8 @@ pair at both thread counts over 20 steps with a sort every 5 steps; stage 2
 times the two best at each pair of sort interval and bank re-layout interval
 over 40 steps (the slow path for particles that drifted out of their tile
 window, the bank conflicts of particles that changed cell, and the sorts
-and re-layouts themselves all count).  Results are cached per GPU model in
+and re-layouts themselves all count); stage 3 (FP32) times the winner
+without the bank-class lane selection.  Results are cached per GPU model in
 a JSON file (``$PICSAR_B200_CACHE`` or ``~/.cache/picsar_b200/autotune.json``).
 
 The reference has no autotuner: its tile counts, vector lengths and
@@ -28,7 +29,7 @@ import torch
 
 from .init import thermal_plasma
 from ._lib import PicsarB200Error
-from .tiled import SUPPORTED_SHAPES, TiledConfig, TiledSim
+from .tiled import SUPPORTED_ACC, SUPPORTED_SHAPES, TiledConfig, TiledSim
 
 THREADS = (128, 256)
 SORT_INTERVALS = (5, 10, 20, 40)
@@ -54,13 +55,22 @@ def _cache_path():
     return os.path.join(os.path.expanduser("~"), ".cache", "picsar_b200", "autotune.json")
 
 
-def _key(order, precision, ppc, sigma, pusher, u_drift=0.0, device_name=None):
+def _key(order, precision, ppc, sigma, pusher, u_drift=0.0, device_name=None, acc=2):
     """Cache key of a job class: GPU model, order, precision, ppc, thermal
-    spread in half-decades, beam drift (2 decimals), pusher."""
+    spread in half-decades, beam drift (2 decimals), pusher, FP32 current
+    accumulator."""
     name = device_name or torch.cuda.get_device_name()
     sb = round(math.log10(max(sigma, 1e-6)) * 2) / 2
     db = f"|d{round(u_drift, 2)}" if u_drift else ""
-    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}{db}|p{pusher}|v4"
+    ab = f"|a{acc}" if precision == "fp32" else ""
+    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}{db}|p{pusher}{ab}|v6"
+
+
+def acc_for(edge, drift, acc):
+    """The FP32 accumulator a (tile edge, margin) shape runs with when `acc`
+    is asked for: `acc` where that shape has it compiled, else the two-word
+    mode every shape has."""
+    return acc if acc in SUPPORTED_ACC.get((edge, drift), (2,)) else 2
 
 
 def proxy_grid(ppc, num_sms, tile=8, ctas_per_sm=2):
@@ -94,12 +104,14 @@ def _time(cfg, order, precision, st, n, steps, pusher):
 
 def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
          shapes=None, threads=THREADS, sort_intervals=SORT_INTERVALS,
-         relayout_intervals=RELAYOUT_INTERVALS, seed=7, u_drift=0.0):
+         relayout_intervals=RELAYOUT_INTERVALS, seed=7, u_drift=0.0, acc=2):
     """Best TiledConfig for jobs of this class, timed on a proxy simulation
     (thermal spread sigma; u_drift > 0: two counter-streaming beams u_x =
-    +-u_drift, as in a two-stream plasma)."""
+    +-u_drift, as in a two-stream plasma).  acc: the FP32 current
+    accumulator the jobs will run with; every candidate is timed with it
+    (acc_for) and the returned config carries it."""
     path = _cache_path()
-    key = _key(order, precision, ppc, sigma, pusher, u_drift)
+    key = _key(order, precision, ppc, sigma, pusher, u_drift, acc=acc)
     if use_cache and os.path.exists(path):
         try:
             with open(path) as f:
@@ -125,7 +137,7 @@ def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
             # a short sort interval, so that shapes are ranked by the kernel
             # rather than by the slow path of particles that left their window
             cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, threads=th, sort_interval=5,
-                              relayout_interval=0)
+                              relayout_interval=0, acc=acc_for(edge, drift, acc))
             try:
                 r = _time(cfg, order, precision, st, n, 20, pusher)
             except (ValueError, RuntimeError, PicsarB200Error) as e:   # not compiled here
@@ -143,11 +155,24 @@ def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
                 if R >= K:
                     continue
                 cfg = TiledConfig(tile=cfg0.tile, drift=cfg0.drift, threads=cfg0.threads,
-                                  sort_interval=K, relayout_interval=R)
+                                  sort_interval=K, relayout_interval=R, acc=cfg0.acc)
                 r = _time(cfg, order, precision, st, n, 40, pusher)
                 table.append((cfg0.tile[0], cfg0.drift, cfg0.threads, K, R, r))
                 if best is None or r > best[1]:
                     best = (cfg, r)
+    # stage 3 (FP32): the winner in one pass, without the bank-class lane
+    # selection (it costs a second pass, which loses where many particles
+    # change cell every step)
+    if precision == "fp32":
+        c1 = best[0]
+        cfg = TiledConfig(tile=c1.tile, drift=c1.drift, threads=c1.threads,
+                          sort_interval=c1.sort_interval, relayout_interval=c1.relayout_interval,
+                          acc=c1.acc, select_lanes=False)
+        r = _time(cfg, order, precision, st, n, 40, pusher)
+        table.append((c1.tile[0], c1.drift, c1.threads, c1.sort_interval, c1.relayout_interval,
+                      r, "one pass"))
+        if r > best[1]:
+            best = (cfg, r)
     res = TuneResult(order, precision, ppc, sigma, best[0], best[1], table)
     if use_cache:
         try:
@@ -186,9 +211,10 @@ def representative(specs):
     return out
 
 
-def tune_ensemble(specs, precision="fp32", use_cache=True):
+def tune_ensemble(specs, precision="fp32", use_cache=True, acc=2):
     """{order: TiledConfig} for an ensemble, one tuning per order present."""
     res = {}
     for o, (ppc, sig, pusher) in representative(specs).items():
-        res[o] = tune(o, precision, ppc=ppc, sigma=sig, pusher=pusher, use_cache=use_cache)
+        res[o] = tune(o, precision, ppc=ppc, sigma=sig, pusher=pusher, use_cache=use_cache,
+                      acc=acc)
     return res

@@ -831,7 +831,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
       if (vz > tez - 1 + D) vz -= nz; else if (vz < -D) vz += nz;
       const bool in_old = vx >= -D && vx <= tex - 1 + D && vy >= -D && vy <= tey - 1 + D &&
                           vz >= -D && vz <= tez - 1 + D;
-      if (SELECT && phase == 0) {
+      if (SELECT && phase == 0 && sj.select_lanes) {
         const bool part = valid && in_old;
         const int hx = ORDER == 2 && ox >= (R)0.5, hy = ORDER == 2 && oy >= (R)0.5,
                   hz = ORDER == 2 && oz >= (R)0.5;

@@ -43,6 +43,7 @@ class TiledJob(C.Structure):
                              "ux_b", "uy_b", "uz_b", "w_b", "pid", "pid_b", "tile_off",
                              "tile_cnt", "ke_tile", "counters", "cell_cnt", "rank_b", "perm",
                              "tile_stats")]
+        + [(n, C.c_int32) for n in ("select_lanes", "reserved")]
     )
 
 
@@ -95,6 +96,7 @@ class TiledConfig:
     sort_interval: int = 20
     relayout_interval: int = 4  # bank-order re-layout of the tiles between sorts (0: none)
     acc: int = 2                # FP32 engine current accumulator (see picsar_b200.h)
+    select_lanes: bool = True   # FP32 engine: distinct bank classes per warp, second pass
 
 
 def h2d_bytes(buf):
@@ -213,6 +215,7 @@ class TiledSim:
         j.ke_tile, j.counters = self.ke_tile.data_ptr(), self.counters.data_ptr()
         j.cell_cnt = self.cell_cnt.data_ptr()
         j.tile_stats = self.tile_stats.data_ptr()
+        j.select_lanes = int(bool(self.cfg.select_lanes))
         self._push_job()
 
     def _jp(self):
