@@ -322,3 +322,102 @@ def test_2d_deck(cuda, tmp_path):
     assert np.abs(jx).max() > 0
     _, kin = _temporal(os.path.join(out, "kinE"))
     assert kin.shape == (4, 1) and (kin > 0).all()
+
+
+HOMOGENEOUS = """ Homogeneous thermal plasma (electrons at 0.1 c, protons at 0.001 c)
+section::main
+ nx = 100
+ ny = 100
+ nz = 100
+ xmin = -20e-6
+ ymin = -20e-6
+ zmin = -20e-6
+ xmax = 20e-6
+ ymax = 20e-6
+ zmax = 20e-6
+ t_max = 2
+ nguardsx = 3
+ nguardsy = 3
+ nguardsz = 3
+ njguardsx = 3
+ njguardsy = 3
+ njguardsz = 3
+end::main
+section::solver
+ nox = 1
+ noy = 1
+ noz = 1
+end::solver
+section::sorting
+ activation = 1
+ shiftx = -0.5
+ shifty = -0.5
+ shiftz = -0.5
+end::sorting
+section::plasma
+ nlab = 1e25
+ gamma0 = 1.
+ pdistr = 1
+end::plasma
+section::species
+ name = electron
+ mass = 1.
+ charge = -1
+ nppcell = 5
+ x_min = -20e-6
+ y_min = -20e-6
+ z_min = -20e-6
+ x_max = 20e-6
+ y_max = 20e-6
+ z_max = 20e-6
+ vth_x = 0.1
+ vth_y = 0.1
+ vth_z = 0.1
+ sorting_period = 10
+end::species
+section::species
+ name = proton
+ mass = 1836.
+ charge = 1
+ nppcell = 5
+ x_min = -20e-6
+ y_min = -20e-6
+ z_min = -20e-6
+ x_max = 20e-6
+ y_max = 20e-6
+ z_max = 20e-6
+ vth_x = 0.001
+ vth_y = 0.001
+ vth_z = 0.001
+ sorting_period = 10
+end::species
+section::temporal
+ frequency = 1
+ kinE = 1
+ exE = 1
+ eyE = 1
+ ezE = 1
+ bxE = 1
+ byE = 1
+ bzE = 1
+end::temporal
+"""
+
+
+def test_homogeneous_plasma_acceptance(cuda, tmp_path):
+    """The reference's homogeneous-plasma acceptance check
+    (Acceptance_testing/Fortran_tests/test_homogeneous_plasma): total
+    energy within 1 % over the run; the step count comes from t_max."""
+    deck = D.read_input_text(HOMOGENEOUS)
+    der = deck.derived()
+    assert der["nsteps"] == int(np.rint(2.0 / (der["w0_l"] * der["dt"])))
+    out = str(tmp_path / "RESULTS")
+    D.run_deck(deck, out_dir=out, seed=5)
+    _, kin = _temporal(os.path.join(out, "kinE"))
+    assert kin.shape == (der["nsteps"], 2)
+    fields = 0.0
+    for name in ("exE", "eyE", "ezE", "bxE", "byE", "bzE"):
+        e = _temporal(os.path.join(out, name))[1][:, 0]
+        fields = fields + (e[1:] + e[:-1]) * 0.5
+    total = kin.T[:, 1:].sum(axis=0) + fields
+    assert (total.max() - total.min()) / total.max() < 1e-2
