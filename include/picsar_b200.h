@@ -306,6 +306,27 @@ int pxrb_particle_bin_sorting(int64_t np, double* xp, double* yp, double* zp, do
                               int64_t scratch_bytes, void* stream);
 
 
+/* Spectral (PSATD) field push of one periodic domain in Fourier space:
+ * replaces push_psaotd_ebfielfs_3d (src/field_solvers/Maxwell/GPSTD_solver/
+ * fourier_psaotd.F90:1538-1643) with the coefficient blocks of
+ * compute_cc_mat_merged_fields (init_kspace_3D.F90:1316-1495).  The field
+ * spectra are DEVICE complex FP64 (interleaved re, im) arrays of
+ * nkx*nky*nkz modes, x fastest: the r2c transforms of the FFT region of
+ * ex..bz (updated in place), jx..jz, rho and rho_old.  kxf, kxb (nkx), kyf,
+ * kyb (nky), kzf, kzb (nkz): DEVICE complex k-vectors (forward, backward
+ * staggering, compute_k_1d); kxc2, kyc2, kzc2: DEVICE |k_centred|^2 per axis;
+ * at1, at2, at3: DEVICE per-mode operators c dt sinc(c|k|dt), cos(c|k|dt),
+ * (1 - cos)/|k|^2 (init_kspace, with its k = 0 values); norm: 1 / (number
+ * of real FFT points), applied to every coefficient as the reference does. */
+int pxrb_psatd_push(int64_t nkx, int64_t nky, int64_t nkz, double* ex, double* ey, double* ez,
+                    double* bx, double* by, double* bz, const double* jx, const double* jy,
+                    const double* jz, const double* rho, const double* rhoold,
+                    const double* kxf, const double* kxb, const double* kyf, const double* kyb,
+                    const double* kzf, const double* kzb, const double* kxc2,
+                    const double* kyc2, const double* kzc2, const double* at1,
+                    const double* at2, const double* at3, double clight, double eps0,
+                    double mu0, double dt, double norm, void* stream);
+
 /* ------------------------------------------------------------------------
  * Tiled engine (B200-native layout): FP32 mixed precision or FP64.
  *

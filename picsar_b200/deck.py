@@ -41,9 +41,12 @@ diagnostics (src/ios/simple_io.F90:236-455, src/diags/diags.F90:253-420,
 847-1300), all under ``<out_dir>/`` (the reference writes ``./RESULTS/``).
 
 Physical constants are the reference's SI values (src/modules/modules.F90:
-57-81).  Not supported (a deck that asks raises ``DeckError``): the laser
-antenna, the spectral (PSATD) solver, PML / absorbing boundaries, different
-shape orders per axis, and (tiled engine) more than one species.
+57-81).  ``l_spectral`` decks run the PSATD push of ``picsar_b200.psatd``
+(3D, plain engine, ``dt = min(dx, dy, dz) / c`` as submain.F90:578-586
+sets it).  Not supported (a deck that asks raises ``DeckError``): the laser
+antenna, the matrix form of the spectral solver (``g_spectral``) and
+distributed FFTs, PML / absorbing boundaries, different shape orders per
+axis, and (tiled engine) more than one species.
 """
 from __future__ import annotations
 
@@ -284,8 +287,6 @@ class Deck:
         """The quantities the reference's initialisation computes from the
         deck for one domain: a dict with cells per axis, dx, dy, dz, dt,
         nsteps, tmax, nc, w0_l and the sorting lengths in metres."""
-        if self.l_spectral:
-            raise DeckError("the spectral (PSATD) solver is not supported")
         nxc = self.nx_global_grid - 1
         nyc = self.ny_global_grid - 1
         nzc = self.nz_global_grid - 1
@@ -298,11 +299,17 @@ class Deck:
         dz = (self.zmax - self.zmin) / nzc
         if self.c_dim == 2:
             dy = HUGE
-            dt = self.dtcoef / (CLIGHT * math.sqrt(1.0 / dx ** 2 + 1.0 / dz ** 2))
+            if self.l_spectral:
+                dt = min(dx, dz) / CLIGHT
+            else:
+                dt = self.dtcoef / (CLIGHT * math.sqrt(1.0 / dx ** 2 + 1.0 / dz ** 2))
         else:
             dy = (self.ymax - self.ymin) / nyc
-            dt = self.dtcoef / (CLIGHT * math.sqrt(1.0 / dx ** 2 + 1.0 / dy ** 2 +
-                                                   1.0 / dz ** 2))
+            if self.l_spectral:
+                dt = min(dx, dy, dz) / CLIGHT
+            else:
+                dt = self.dtcoef / (CLIGHT * math.sqrt(1.0 / dx ** 2 + 1.0 / dy ** 2 +
+                                                       1.0 / dz ** 2))
         nc = self.nlab * self.g0
         w0_l = ECHARGE * math.sqrt(nc / (self.g0 * EMASS * EPS0))
         if self.nsteps == 0:
@@ -820,8 +827,11 @@ def build(deck, engine="plain", precision="fp64", device="cuda", seed=0, tiled_c
     (c_dim 2) in SI units with its species loaded.  Returns (module, derived)."""
     if deck.antenna:
         raise DeckError("the laser antenna is not supported")
-    if deck.l_spectral or deck.g_spectral:
-        raise DeckError("the spectral (PSATD) solver is not supported")
+    if deck.g_spectral or deck.fftw_with_mpi or deck.p3dfft_flag:
+        raise DeckError("spectral variants other than the local-FFT PSATD push are not "
+                        "supported (g_spectral, distributed FFTs)")
+    if deck.l_spectral and (deck.c_dim != 3 or engine != "plain"):
+        raise DeckError("the spectral (PSATD) solver runs 3D decks on the plain engine")
     if deck.absorbing_bcs_x or deck.absorbing_bcs_y or deck.absorbing_bcs_z or \
             deck.nx_pml or deck.ny_pml or deck.nz_pml:
         raise DeckError("PML / absorbing field boundaries are not supported")
@@ -858,6 +868,7 @@ def build(deck, engine="plain", precision="fp64", device="cuda", seed=0, tiled_c
                          precision=precision, tiled_config=tiled_config)
         m.norderx, m.nordery, m.norderz = deck.norderx, deck.nordery, deck.norderz
         m.l_lower_order_in_v = deck.l_lower_order_in_v
+        m.l_spectral, m.l_staggered = bool(deck.l_spectral), bool(deck.l_staggered)
         if engine == "plain":
             m.sorting_activated = deck.sorting_activated
             m.sorting_dx, m.sorting_dy, m.sorting_dz = der["sorting_d"]

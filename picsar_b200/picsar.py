@@ -43,6 +43,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import psatd as _psatd
 from ._lib import PicsarB200Error
 
 # ---------------------------------------------------------------------------
@@ -203,6 +204,11 @@ class PicsarModule:
         # Maxwell solver (modules.F90 fields): FDTD order per axis, nodal grid
         self.norderx = self.nordery = self.norderz = 2
         self.l_nodalgrid = False
+        # spectral (PSATD) solver instead of Yee (fields: l_spectral,
+        # l_staggered); norderx.. then give its stencil orders (0: infinite)
+        self.l_spectral = False
+        self.l_staggered = True
+        self._psatd = None
         self.nxs = self.nys = self.nzs = 0
         self.particle_pusher = int(particle_pusher)
         self.l_lower_order_in_v = True
@@ -481,10 +487,67 @@ class PicsarModule:
         self.pxrdepose_rho_on_grid()
         self.charge_bcs()
 
+    def push_psatd_ebfield(self):
+        """The spectral field push (maxwell_solver_manager.F90:574-642, local
+        FFT): E and B over the FFT region advanced by one analytical step
+        from J, rho and rho_old (picsar_b200.psatd)."""
+        if self._tiled is not None:
+            raise PicsarB200Error("the spectral solver runs on the plain engine")
+        key = (self.dx, self.dy, self.dz, self.dt, self.norderx, self.nordery, self.norderz,
+               bool(self.l_staggered), self.clight, self.eps0, self.mu0)
+        if self._psatd is None or self._psatd[0] != key:
+            g = (self.nxguards, self.nyguards, self.nzguards)
+            solver = _psatd.PsatdSolver((self.nx, self.ny, self.nz), g,
+                                        (self.dx, self.dy, self.dz), self.dt,
+                                        (self.norderx, self.nordery, self.norderz),
+                                        bool(self.l_staggered), self.clight, self.eps0,
+                                        self.mu0, device=self.device)
+            self._psatd = (key, solver)
+        if "rhoold" not in self._grids:
+            self._grids["rhoold"] = torch.zeros_like(self.rho)
+        self._psatd[1].push(self.ex, self.ey, self.ez, self.bx, self.by, self.bz, self.jx,
+                            self.jy, self.jz, self.rho, self._grids["rhoold"],
+                            stream=_stream())
+
+    @property
+    def rhoold(self):
+        """rho of the previous step (spectral solver)."""
+        if "rhoold" not in self._grids:
+            self._grids["rhoold"] = torch.zeros_like(self.rho)
+        return self._grids["rhoold"]
+
+    def _step_spectral(self, nst, diags):
+        """PIC loop of src/submain.F90:101-150 with l_spectral: rho and
+        rho_old start at zero; per step rho_old = rho and rho is deposited
+        before the sort and the current deposition, then the PSATD push."""
+        self.rho.zero_()
+        self.rhoold.zero_()
+        for _ in range(nst):
+            self.field_gathering_plus_particle_pusher()
+            self.particle_bcs()
+            self.rhoold.copy_(self.rho)
+            self.pxrdepose_rho_on_grid()
+            self.charge_bcs()
+            self.pxr_particle_sorting()
+            self.pxrdepose_currents_on_grid_jxjyjz()
+            self.current_bcs()
+            self.push_psatd_ebfield()
+            self.efield_bcs()
+            self.bfield_bcs()
+            if diags:
+                self.calc_diags()
+            self.it += 1
+
     def step(self, nst=1, diags=False):
-        """PIC loop of src/submain.F90:104-195 (Yee solver, l_plasma).  Tiled
-        engine: one fused particle kernel and three Yee launches per step,
-        with the engine's own sort and re-layout schedule."""
+        """PIC loop of src/submain.F90:104-195 (Yee solver, or the spectral
+        solver when l_spectral, l_plasma).  Tiled engine: one fused particle
+        kernel and three Yee launches per step, with the engine's own sort and
+        re-layout schedule."""
+        if self.l_spectral:
+            if self._tiled is not None:
+                raise PicsarB200Error("the spectral solver runs on the plain engine")
+            self._step_spectral(nst, diags)
+            return
         if self._tiled is not None:
             for _ in range(nst):
                 self._tiled.step()

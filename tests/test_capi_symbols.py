@@ -34,6 +34,7 @@ def test_python_signatures_cover_header():
     from picsar_b200 import _lib
     import picsar_b200.ensemble  # noqa: F401  (these modules register their signatures)
     import picsar_b200.picsar  # noqa: F401
+    import picsar_b200.psatd  # noqa: F401
     import picsar_b200.tiled  # noqa: F401
     declared = _declared()
     missing = sorted(declared - set(_lib.exported_symbols()))
