@@ -99,3 +99,33 @@ def test_spectral_steps_against_oracle_push(cuda):
     for c in ("part_x", "part_ux", "part_uz"):
         assert rel_l2(getattr(a.species[0], c).cpu().numpy(),
                       getattr(b.species[0], c).cpu().numpy()) <= 1e-12, c
+
+
+@pytest.mark.parametrize("norder", [2, 8, 0])
+def test_vacuum_plane_wave_keeps_its_energy(cuda, norder):
+    """A vacuum plane wave along z whose wavelength divides both the domain
+    (32 cells) and the FFT extent (32 + 2 * 8 guards): 64 spectral pushes
+    (with the periodic field exchanges) keep its E^2 + B^2 to 1e-12 and keep
+    it uniform in x and y."""
+    import math
+    n, g = 32, 8
+    m = P.PicsarModule(n, n, n, nguards=g, dx=1.0, dy=1.0, dz=1.0, dt=0.5)
+    m.l_spectral = True
+    m.norderx = m.nordery = m.norderz = norder
+    z = torch.arange(-g, n + g + 1, dtype=torch.float64, device="cuda")
+    k = 2 * math.pi / 16
+    full = (n + 1 + 2 * g,) * 3
+    m.ex.copy_(torch.cos(k * z)[None, None, :].expand(full))
+    m.by.copy_(torch.cos(k * (z + 0.5) + k * 0.25)[None, None, :].expand(full))
+    inner = (slice(g, g + n),) * 3
+    energy = lambda: float((m.ex[inner] ** 2).sum() + (m.by[inner] ** 2).sum() +
+                           (m.ez[inner] ** 2).sum() + (m.bx[inner] ** 2).sum())
+    e0 = energy()
+    for _ in range(64):
+        m.push_psatd_ebfield()
+        m.efield_bcs()
+        m.bfield_bcs()
+    torch.cuda.synchronize()
+    assert abs(energy() / e0 - 1.0) < 1e-12
+    ex = m.ex[inner]
+    assert float((ex - ex[:1, :1, :]).abs().max()) < 1e-12
