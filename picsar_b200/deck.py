@@ -163,7 +163,9 @@ class Species:
 
 @dataclass
 class ParticleDump:
-    """One ``section::particle_dump`` (parsed; particle dumps are not written)."""
+    """One ``section::particle_dump``: every diag_period iterations the
+    particles of one species inside the (strict) position and momentum
+    ranges are written (write_particles_to_file)."""
     ispecies: int = -1
     dump_x_min: float = 0.0
     dump_x_max: float = 0.0
@@ -822,6 +824,43 @@ def _output_fields(m, deck, grids, it, out_dir):
     return written
 
 
+def _output_particles(m, deck, it, out_dir):
+    """The particle dumps of write_particles_to_file (simple_io.F90:601-697,
+    one domain): ``<species>_it_<it>`` holding x, y, z, ux, uy, uz and the
+    weight of the selected particles, each as a block of FP64 values.  The
+    selection is strict on every bound (get_particles_to_dump,
+    :709-761); the reference marks its mask at tile-local indices but reads
+    it at global ones, which agree with one tile, the case here."""
+    import torch
+    written = []
+    lab = _step_label(it)
+    for dp in deck.particle_dumps:
+        if dp.diag_period < 1 or it % dp.diag_period != 0 or dp.ispecies < 0:
+            continue
+        sp = m.species[dp.ispecies]
+        cols = [getattr(sp, c).to(torch.float64) for c in
+                ("part_x", "part_y", "part_z", "part_ux", "part_uy", "part_uz", "pid_w")]
+        x, y, z, ux, uy, uz, _ = cols
+        keep = ((x > dp.dump_x_min) & (x < dp.dump_x_max) & (y > dp.dump_y_min) &
+                (y < dp.dump_y_max) & (z > dp.dump_z_min) & (z < dp.dump_z_max) &
+                (ux > dp.dump_ux_min) & (ux < dp.dump_ux_max) & (uy > dp.dump_uy_min) &
+                (uy < dp.dump_uy_max) & (uz > dp.dump_uz_min) & (uz < dp.dump_uz_max))
+        path = os.path.join(out_dir, f"{sp.name}_it_{lab}")
+        with open(path, "wb") as f:
+            for c in cols:
+                f.write(c[keep].cpu().numpy().astype("<f8").tobytes())
+        written.append(path)
+    return written
+
+
+def read_particle_dump(path):
+    """{x, y, z, ux, uy, uz, w} of a particle dump file."""
+    v = np.fromfile(path, dtype="<f8")
+    n = v.size // 7
+    return {c: v[i * n:(i + 1) * n] for i, c in enumerate(("x", "y", "z", "ux", "uy", "uz",
+                                                            "w"))}
+
+
 def build(deck, engine="plain", precision="fp64", device="cuda", seed=0, tiled_config=None):
     """The deck's simulation: a ``PicsarModule`` (c_dim 3) or ``PicsarModule2D``
     (c_dim 2) in SI units with its species loaded.  Returns (module, derived)."""
@@ -906,6 +945,8 @@ def run_deck(deck, out_dir="RESULTS", engine="plain", precision="fp64", device="
         else:
             m.step(1, diags=rho_on)          # calc_diags: rho deposition + charge_bcs
         dumps += _output_fields(m, deck, grids, it, out_dir)
+        if deck.c_dim == 3:
+            dumps += _output_particles(m, deck, it, out_dir)
         if temporal.due(it):
             temporal.write(_temporal_values(m, deck, grids, need))
     return m, {"dumps": dumps, "nsteps": steps, "derived": der}

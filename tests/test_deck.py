@@ -107,6 +107,17 @@ def test_reader_rules():
         D.read_input_text(BASE.replace(" nx = 17\n", " nx = 1x\n"))
 
 
+def test_particle_dump_section():
+    text = BASE + ("section::particle_dump\n species_name = electron\n diag_period = 5\n"
+                   " dump_ux_min = -1e9\nend::particle_dump\n")
+    d = D.read_input_text(text)
+    dp, = d.particle_dumps
+    assert dp.ispecies == 0 and dp.diag_period == 5 and dp.dump_ux_min == -1e9
+    # bounds not given default to the domain read so far and to 1e7..1e9
+    assert dp.dump_x_min == d.xmin and dp.dump_z_max == d.zmax
+    assert dp.dump_uy_min == 1e7 and dp.dump_uz_max == 1e9
+
+
 def test_nsteps_from_t_max():
     d = D.read_input_text(BASE.replace(" nsteps = 12\n", " t_max = 0.5\n"))
     der = d.derived()

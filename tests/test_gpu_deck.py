@@ -216,6 +216,13 @@ section::temporal
  divE-rho = 1
  rho = 1
 end::temporal
+section::particle_dump
+ species_name = electron
+ dump_ux_min = -1e9
+ dump_uy_min = -1e9
+ dump_uz_min = -1e9
+ diag_period = 1
+end::particle_dump
 """
 
 
@@ -261,6 +268,11 @@ def test_small_deck_against_oracle(cuda, tmp_path, engine, order):
         assert abs(records["bzE"][it, 0] - bze) <= 1e-12 * bze
         rn = math.sqrt(float((f["rho"][one] ** 2).sum()))
         assert abs(records["rho"][it, 0] - rn) <= 1e-12 * rn
+        # particle dump: every particle (the ranges hold them all), add order
+        pd = D.read_particle_dump(os.path.join(out, f"electron_it_{it}"))
+        assert len(pd["x"]) == len(q["x"])
+        for c in ("x", "y", "z", "ux", "uy", "uz", "w"):
+            assert rel_l2(pd[c], q[c]) <= 1e-12, (c, it)
 
 
 PLANE_2D = """section::cpusplit
