@@ -70,12 +70,20 @@ DEPOSIT_UPDATES = {1: 12, 2: 54, 3: 144}
 SMEM_RATE = {"lds": 0.88, "atoms": 0.61}
 
 
+def smem_per_particle(order, acc):
+    """(window loads, accumulator atomics) per particle of the fused particle
+    kernel.  The cell-grouped kernel (acc 4) loads each window value once per
+    group of four particles of a cell and updates a J node once per pair."""
+    if acc == 4:
+        return GATHER_POINTS[order] / 4.0, DEPOSIT_UPDATES[order] / 2.0
+    return GATHER_POINTS[order], DEPOSIT_UPDATES[order] * (2 if acc == 2 else 1)
+
+
 def smem_floor_ms(order, acc, particles, sms, clock_mhz):
     """Lower bound of the fused particle kernel's time set by shared-memory
     instruction throughput (loads and accumulator atomics, conflict-free)."""
-    words = 2 if acc == 2 else 1
-    clk_per_warp = (GATHER_POINTS[order] / SMEM_RATE["lds"] +
-                    DEPOSIT_UPDATES[order] * words / SMEM_RATE["atoms"])
+    lds, atoms = smem_per_particle(order, acc)
+    clk_per_warp = lds / SMEM_RATE["lds"] + atoms / SMEM_RATE["atoms"]
     return particles / 32.0 * clk_per_warp / sms / (clock_mhz * 1e6) * 1e3
 GRID_BYTES_PER_CELL = {0: (24 + 48), 1: (48 + 48)}        # E,B read + J FP64 read-modify-write
 
@@ -510,8 +518,9 @@ def _smem_roofline(wl, prec, cfg, N, kern_ms, clk):
     mhz = (clk or {}).get("sm_mhz") or 1965.0
     floor = smem_floor_ms(wl["order"], cfg.acc, N, sms, mhz)
     return {"bound": "shared-memory instructions", "floor_ms": floor, "kernel_ms": kern_ms,
-            "frac": floor / kern_ms, "gather_points": GATHER_POINTS[wl["order"]],
-            "accumulator_updates": DEPOSIT_UPDATES[wl["order"]] * (2 if cfg.acc == 2 else 1),
+            "frac": floor / kern_ms,
+            "window_loads_per_particle": smem_per_particle(wl["order"], cfg.acc)[0],
+            "accumulator_atomics_per_particle": smem_per_particle(wl["order"], cfg.acc)[1],
             "rates_warp_inst_per_clk_sm": SMEM_RATE, "sm_mhz": mhz}
 
 

@@ -383,7 +383,11 @@ typedef struct pxrb_tiled_job {
                                                others to a second, class-bucketed pass;
                                                0 = one pass (faster when many particles
                                                change cell per step) */
-  int32_t reserved;                         /* 0 */
+  int32_t cell_order;                       /* 1 = the sort leaves each tile's particles
+                                               in cell order (the layout of the
+                                               cell-grouped kernel, acc 4) and the
+                                               bank re-layout leaves them in place;
+                                               0 = bank order */
 } pxrb_tiled_job;
 
 /* Tile shapes: cubic tiles of edge tx = ty = tz = `tile` in {4, 8} with window

@@ -365,6 +365,13 @@ __global__ void __launch_bounds__(TM_WARPS * 32) k_tile_map(const Job* __restric
   if (t >= ntl) return;                       // whole warp
   const int b0 = J.tile_off[t], b1 = J.tile_off[t + 1];
   if (b0 == b1) return;
+  if (J.cell_order) {
+    // cell order: the sort's permutation as it is; a re-layout keeps the
+    // current order (the cell-grouped kernel groups by cell itself)
+    for (int i = b0 + lane; i < b1; i += 32)
+      J.cell_b[i] = CELL_MAJOR ? (uint32_t)J.perm[i] : (uint32_t)i;
+    return;
+  }
   const int T = J.tx, D = J.drift, nx = J.nx, ny = J.ny, nz = J.nz;
   const int L = J.order == 1 ? 0 : 1, H = J.order == 1 ? 1 : 2;
   const int W = T + 2 * D + L + H;
@@ -776,6 +783,8 @@ int64_t smem_bytes(int order, int prec, int acc, int tx, int ty, int tz, int dri
   i64 r = prec ? 8 : 4;
   i64 a = acc == 3 ? 8 : 4, nw = acc == 2 ? 2 : 1;
   const i64 hb = tx + 2 * drift;      // next-step occupancy histogram (fixed point)
+  if (acc == 4)                       // cell-grouped kernel: + per-cell counts and order
+    return V * 36 + hb * hb * hb * 12 + 8 + ((hb * hb * hb * 2 + 15) / 16) * 16;
   return V * (6 * r + 3 * a * nw) + ((acc == 1 || acc == 2) ? hb * hb * hb * 4 : 0);
 }
 

@@ -1,5 +1,5 @@
 // Instantiations of the fused particle kernel for shape order 3.
-#include "pxr_tiled_kernel.cuh"
+#include "pxr_cell_kernel.cuh"
 
 namespace pxrt {
 template <typename R, int ORDER, int T, int D, int MODE>
@@ -23,6 +23,12 @@ int launch_shape(int tile, int drift, int mode, const Job* jobs, const int2* wor
   if (tile == T_ && drift == D_ && mode == M_)                                              \
     return launch_step<R, ORDER, T_, D_, M_>(jobs, work, nwork, nwork_dev, ctr, threads,    \
                                              ctas, smem, s);
+  if (mode == 4) {       // cell-grouped kernel (FP32, int32 fixed point)
+    if (sizeof(R) != 4) return PXRB_EUNSUPPORTED;
+    if (tile == 8 && drift == 1)
+      return launch_cell<ORDER, 8, 1>(jobs, work, nwork, nwork_dev, ctr, threads, ctas, smem, s);
+    return PXRB_EUNSUPPORTED;
+  }
   if (sizeof(R) == 8) {
     PXRB_TD(8, 1, 3)
     PXRB_TD(8, 0, 3)

@@ -33,7 +33,7 @@ import torch
 
 from . import _lib
 from .init import thermal_plasma
-from .tiled import TiledConfig, TiledJob, TiledSim, _stream, h2d
+from .tiled import TiledConfig, TiledJob, TiledSim, _stream, h2d, launch_threads
 
 _lib.register({"pxrb_tiled_sort_batch": "p I I I i s", "pxrb_tiled_relayout": "p I I I i s"})
 
@@ -282,7 +282,7 @@ class Ensemble:
             ctas = min(grp.nwork, self.num_sms * cfg.ctas_per_sm)
             _lib.call("pxrb_tiled_particle_step", jd, grp.order, self.prec, cfg.tile[0],
                       cfg.drift, grp.acc, grp.work.data_ptr(), grp.nwork, None,
-                      grp.ctr.data_ptr(), cfg.threads, ctas, grp.smem, s)
+                      grp.ctr.data_ptr(), launch_threads(cfg, grp.acc), ctas, grp.smem, s)
         co = self.cell_off.data_ptr()
         _lib.call("pxrb_tiled_push_b", jd, self.njobs, self.prec, co, self.total_cells, 0.5, s)
         _lib.call("pxrb_tiled_push_e", jd, self.njobs, self.prec, co, self.total_cells, 1, s)
@@ -347,7 +347,7 @@ class Ensemble:
                 if K > 0 and self.it % K == 0:
                     self._run(("sort", grp.order), lambda grp=grp: self._launch_sort(grp))
                     self.launches += 7
-                elif R > 0 and self.it % R == 0 and grp.max_np > 0:
+                elif R > 0 and self.it % R == 0 and grp.max_np > 0 and grp.acc != 4:
                     self._run(("relayout", grp.order), lambda grp=grp: self._launch_relayout(grp))
                     self.launches += 3
 
@@ -384,7 +384,7 @@ class Ensemble:
                 ctas = min(grp.nwork, self.num_sms * cfg.ctas_per_sm)
                 _lib.call("pxrb_tiled_particle_step", jd, grp.order, self.prec, cfg.tile[0],
                           cfg.drift, grp.acc, grp.work.data_ptr(), grp.nwork, None,
-                          grp.ctr.data_ptr(), cfg.threads, ctas, grp.smem, _stream())
+                          grp.ctr.data_ptr(), launch_threads(cfg, grp.acc), ctas, grp.smem, _stream())
             ev[1].record(s)
             co = self.cell_off.data_ptr()
             _lib.call("pxrb_tiled_push_b", jd, self.njobs, self.prec, co, self.total_cells, 0.5,

@@ -43,7 +43,7 @@ class TiledJob(C.Structure):
                              "ux_b", "uy_b", "uz_b", "w_b", "pid", "pid_b", "tile_off",
                              "tile_cnt", "ke_tile", "counters", "cell_cnt", "rank_b", "perm",
                              "tile_stats")]
-        + [(n, C.c_int32) for n in ("select_lanes", "reserved")]
+        + [(n, C.c_int32) for n in ("select_lanes", "cell_order")]
     )
 
 
@@ -83,7 +83,15 @@ SUPPORTED_SHAPES = {(8, 1), (8, 0), (8, 2), (4, 1), (4, 0)}
 # ... and those of the FP64 engine
 SUPPORTED_SHAPES_FP64 = {(8, 1), (8, 0), (4, 1), (4, 0)}
 # accumulator modes compiled for the FP32 engine per shape (FP64 engine: mode 3)
-SUPPORTED_ACC = {(8, 1): (0, 1, 2), (8, 2): (1, 2), (4, 1): (1, 2)}
+SUPPORTED_ACC = {(8, 1): (0, 1, 2, 4), (8, 2): (1, 2), (4, 1): (1, 2)}
+# mode 4: the cell-grouped kernel (int32 fixed point like mode 1; FP32, shape
+# orders 1 and 3) runs CTAs of at most this many threads
+CELL_THREADS = 192
+
+
+def launch_threads(cfg, acc):
+    """CTA size of the particle kernel for a configuration and accumulator."""
+    return min(cfg.threads, CELL_THREADS) if acc == 4 else cfg.threads
 
 
 @dataclass
@@ -185,6 +193,8 @@ class TiledSim:
         self.acc = 3 if self.prec == 1 else cfg.acc
         if self.prec == 0 and self.acc not in SUPPORTED_ACC.get((tile[0], cfg.drift), (2,)):
             raise ValueError(f"accumulator mode {self.acc} not compiled for this tile shape")
+        if self.acc == 4 and self.order == 2:
+            raise ValueError("the cell-grouped kernel (mode 4) takes shape orders 1 and 3")
         self.smem = smem_bytes(self.order, self.prec, self.acc, tile, cfg.drift)
         props = torch.cuda.get_device_properties(self.device)
         self.num_sms = props.multi_processor_count
@@ -216,6 +226,7 @@ class TiledSim:
         j.cell_cnt = self.cell_cnt.data_ptr()
         j.tile_stats = self.tile_stats.data_ptr()
         j.select_lanes = int(bool(self.cfg.select_lanes))
+        j.cell_order = int(self.acc == 4)
         self._push_job()
 
     def _jp(self):
@@ -341,7 +352,7 @@ class TiledSim:
         ctas = min(self.ntiles, self.num_sms * self.cfg.ctas_per_sm)
         _lib.call("pxrb_tiled_particle_step", self.job_dev.data_ptr(), self.order, self.prec,
                   self.tile[0], self.cfg.drift, self.acc, self.work.data_ptr(), self.ntiles, None, self.ctr.data_ptr(),
-                  self.cfg.threads, ctas, self.smem, _stream())
+                  launch_threads(self.cfg, self.acc), ctas, self.smem, _stream())
         self.launches += 1
 
     def push_b(self, frac=0.5):
@@ -384,8 +395,9 @@ class TiledSim:
         between sorts."""
         if self.cfg.sort_interval > 0 and self.it % self.cfg.sort_interval == 0:
             self.sort()
-        elif self.cfg.relayout_interval > 0 and self.it % self.cfg.relayout_interval == 0:
-            self.relayout()
+        elif (self.cfg.relayout_interval > 0 and self.acc != 4
+              and self.it % self.cfg.relayout_interval == 0):
+            self.relayout()      # (the cell-grouped kernel orders particles itself)
 
     # ----------------------------------------------------------- diagnostics
     def diagnostics(self, gauss=True, to_host=True, pull=True):
