@@ -362,7 +362,7 @@ def run_ours(args, emit=True):
         r = autotune.tune(wl["order"], args.precision, ppc=wl["ppc"], sigma=wl["sigma"],
                           u_drift=wl.get("u_drift", 0.0),
                           pusher=wl["pusher"], acc=args.acc)
-        cfg = _with_acc({0: r.config}, args.acc)[0]
+        cfg = _with_acc({wl["order"]: r.config}, args.acc)[wl["order"]]
         tuned = {"proxy_rate": r.rate, "cached": r.cached}
     st = _initial_state(wl, 1234 + rank)
     N = st.np
@@ -947,7 +947,7 @@ def _with_acc(configs, acc):
     from picsar_b200.tiled import TiledConfig
     out = {}
     for o, c in configs.items():
-        a = acc_for(c.tile[0], c.drift, acc)
+        a = acc_for(c.tile[0], c.drift, acc, o)
         out[o] = TiledConfig(tile=c.tile, drift=c.drift, threads=c.threads,
                              ctas_per_sm=c.ctas_per_sm, sort_interval=c.sort_interval, acc=a,
                              relayout_interval=c.relayout_interval,

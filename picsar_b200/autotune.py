@@ -66,11 +66,18 @@ def _key(order, precision, ppc, sigma, pusher, u_drift=0.0, device_name=None, ac
     return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}{db}|p{pusher}{ab}|v6"
 
 
-def acc_for(edge, drift, acc):
+def acc_for(edge, drift, acc, order=3):
     """The FP32 accumulator a (tile edge, margin) shape runs with when `acc`
     is asked for: `acc` where that shape has it compiled, else the two-word
-    mode every shape has."""
-    return acc if acc in SUPPORTED_ACC.get((edge, drift), (2,)) else 2
+    mode every shape has.  Mode 4 (the cell-grouped kernel, shape orders 1
+    and 3) falls back to mode 1, the same int32 accumulator with one
+    particle per thread."""
+    if acc == 4 and order == 2:
+        acc = 1
+    ok = SUPPORTED_ACC.get((edge, drift), (2,))
+    if acc in ok:
+        return acc
+    return 1 if acc == 4 and 1 in ok else 2
 
 
 def proxy_grid(ppc, num_sms, tile=8, ctas_per_sm=2):
@@ -137,7 +144,7 @@ def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
             # a short sort interval, so that shapes are ranked by the kernel
             # rather than by the slow path of particles that left their window
             cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, threads=th, sort_interval=5,
-                              relayout_interval=0, acc=acc_for(edge, drift, acc))
+                              relayout_interval=0, acc=acc_for(edge, drift, acc, order))
             try:
                 r = _time(cfg, order, precision, st, n, 20, pusher)
             except (ValueError, RuntimeError, PicsarB200Error) as e:   # not compiled here

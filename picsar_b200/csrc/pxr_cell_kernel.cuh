@@ -159,12 +159,16 @@ __device__ __forceinline__ void cg_deposit(int* base, const f2_t (*t0)[4], const
 constexpr int CG_THREADS = 192;
 constexpr int CG_MINB = 2;
 
+// Entries of the per-tile level table of the group order (levels beyond it
+// are placed by a loop over the 32 classes).
+constexpr int CG_LT = 256;
+
 // Dynamic shared memory of the cell-grouped kernel: E/B window, int32 J
-// window, the next step's cell occupancy, per-cell counts and first slots,
-// and the bank-cycling cell order.
+// window, the next step's cell occupancy, per-cell counts and group
+// prefixes, the window cells ordered by bank class, and the level table.
 __host__ __device__ constexpr int cg_smem_bytes(int T, int D, int V) {
-  return V * (6 * 4 + 3 * 4) + (T + 2 * D) * (T + 2 * D) * (T + 2 * D) * 4 * 3 + 8 +
-         (((T + 2 * D) * (T + 2 * D) * (T + 2 * D) * 2 + 15) / 16) * 16;
+  return V * (6 * 4 + 3 * 4) + (T + 2 * D) * (T + 2 * D) * (T + 2 * D) * 4 * 3 + 4 +
+         (((T + 2 * D) * (T + 2 * D) * (T + 2 * D) * 2 + 15) / 16) * 16 + CG_LT * 8;
 }
 
 // ---------------------------------------------------------------------------
@@ -173,19 +177,23 @@ __host__ __device__ constexpr int cg_smem_bytes(int T, int D, int V) {
 //   1. the E/B window is staged with cp.async while the tile's particles are
 //      counted per window cell (one shared atomic each; particles outside
 //      the window go to one more bucket), and the counts are scanned;
-//   2. each window cell of n particles makes ceil(n/4) groups; the groups
-//      are numbered round by round (every cell's first group, then every
-//      second group, ...), and within a round in an order of the cells that
-//      cycles through the 32 shared-memory bank classes, so the 32 groups of
-//      a warp load and update distinct banks;
+//   2. each window cell of n particles makes ceil(n/4) groups; a group's
+//      bank class is its cell's (the bank of the cell's window address, where
+//      its gather loads and deposit atomics start); the groups are numbered
+//      within their class (level) and laid out by (level, class), so 32
+//      consecutive groups - a warp's - sit in distinct banks until classes
+//      run out (the sort's particle layout, applied to groups);
 //   3. each thread takes a group: gather, push, position, and the summed
 //      deposit of the particles that stay in the cell; particles that change
 //      cell join k_tile_step's node-change queue (window) or deposit on the
 //      global grid; particles outside the window take the global path.
 // Scratch, all in the tile's range of the sort buffers that are free between
-// sorts: uy_b (window cell and rank per particle), perm (particles in cell
-// order), ux_b (the groups), rank_b / cell_b / ox_b / oy_b / oz_b (the
-// node-change queue, as in k_tile_step).
+// sorts: w_b (window cell and rank per particle); perm, ux_b, uy_b, uz_b (the
+// four particle slots of each group, in group order, so a warp reads its
+// groups' slots with coalesced loads: tile-relative particle index | window
+// cell << 21, -1 for an empty slot; particles outside the window follow the
+// groups in perm); rank_b / cell_b / ox_b / oy_b / oz_b (the node-change
+// queue, as in k_tile_step).  A tile holds fewer than 2^21 particles.
 // ---------------------------------------------------------------------------
 template <int ORDER, int T, int D>
 __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
@@ -205,8 +213,10 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
   A* Js = reinterpret_cast<A*>(smem_raw + (size_t)6 * V * sizeof(R));
   int* nh = Js + 3 * V;                 // next step's occupancy of the window cells
   int* s_cnt = nh + NH;                 // particles per window cell; [NH]: outside
-  int* s_start = s_cnt + NH + 1;        // their first slot in cell order
-  unsigned short* s_sig = reinterpret_cast<unsigned short*>(s_start + NH + 1);
+  int* s_pre = s_cnt + NH + 1;          // groups of the cell's class before its own
+  unsigned short* s_tau = reinterpret_cast<unsigned short*>(s_pre + NH);  // by class
+  int* s_lvP = reinterpret_cast<int*>(smem_raw + cg_smem_bytes(T, D, V) - CG_LT * 8);
+  unsigned* s_lvM = reinterpret_cast<unsigned*>(s_lvP + CG_LT);
   __shared__ int s_have;
   __shared__ Job sj;
   __shared__ int s_item;
@@ -214,7 +224,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
   __shared__ float s_max[5][CG_THREADS / 32];
   __shared__ double s_red[CG_THREADS / 32];
   __shared__ int s_scan[4][CG_THREADS / 32];
-  __shared__ int s_ncls[32];
+  __shared__ int s_ncls[32];            // window cells per class
+  __shared__ int s_coff[33];            // their start in s_tau
+  __shared__ int s_G[32];               // groups per class
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   auto cls = [](int h) {
     const int hx = h % HB, hy = (h / HB) % HB, hz = h / (HB * HB);
@@ -226,27 +238,24 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
     const int q = r % V, c = q / SZ, b = (q - c * SZ) / SY, a = q - c * SZ - b * SY;
     if (a >= W || b >= W) Fs[r] = (R)0;
   }
-  // the window cells in bank-cycling order: numbered within their class in
-  // cell order (level), then ordered by (level, class)
+  // the window cells ordered by (class, cell), once per CTA
   if (threadIdx.x < 32) s_ncls[threadIdx.x] = 0;
   __syncthreads();
   for (int h = threadIdx.x; h < NH; h += blockDim.x) atomicAdd(&s_ncls[cls(h)], 1);
   __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int c = 0; c < 32; ++c) { s_coff[c] = t; t += s_ncls[c]; }
+    s_coff[32] = t;
+  }
+  __syncthreads();
   for (int q = wid; q < 32; q += nwarps) {
-    int lev = 0;
+    int lev = s_coff[q];
     for (int h0 = 0; h0 < NH; h0 += 32) {
       const int h = h0 + lane;
       const bool m = h < NH && cls(h) == q;
       const unsigned b = __ballot_sync(0xffffffffu, m);
-      if (m) {
-        const int l = lev + __popc(b & ((1u << lane) - 1u));
-        int pos = 0;
-        for (int c = 0; c < 32; ++c) {
-          const int n = s_ncls[c];
-          pos += min(n, l) + (c < q && n > l ? 1 : 0);
-        }
-        s_sig[pos] = (unsigned short)h;
-      }
+      if (m) s_tau[lev + __popc(b & ((1u << lane) - 1u))] = (unsigned short)h;
       lev += __popc(b);
     }
   }
@@ -311,7 +320,11 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
     uint32_t* cellp = sj.cell;
     R *oxp = (R*)sj.ox, *oyp = (R*)sj.oy, *ozp = (R*)sj.oz;
     R *uxp = (R*)sj.ux, *uyp = (R*)sj.uy, *uzp = (R*)sj.uz;
-    int* keyrank = reinterpret_cast<int*>(sj.uy_b);
+    int* keyrank = reinterpret_cast<int*>(sj.w_b);
+    int* gs0 = sj.perm + pbeg;
+    int* gs1 = reinterpret_cast<int*>(sj.ux_b) + pbeg;
+    int* gs2 = reinterpret_cast<int*>(sj.uy_b) + pbeg;
+    int* gs3 = reinterpret_cast<int*>(sj.uz_b) + pbeg;
     // ---- particles per window cell (+ the fixed-point bounds after a sort) --
     {
       int* hist = reinterpret_cast<int*>(Js) + 2 * V;   // zero; re-zeroed below
@@ -344,63 +357,65 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
         umax2 = stats[0]; wmax = stats[1]; cmax = stats[2];
       }
     }
-    // ---- scan in bank-cycling cell order: slots, and the groups' rounds ----
-    // per cell: n particles, g = ceil(n/4) groups; rounds 0..3 are numbered
-    // by flags (g > k) in 16-bit fields, groups beyond the fourth of a cell
-    // (dense cells) follow all rounds, cell by cell.
-    int NI;
-    {
-      const int per = (NH + blockDim.x - 1) / blockDim.x;
-      const int j0 = threadIdx.x * per, j1 = min(j0 + per, NH);
-      int v0 = 0, v1 = 0, v2 = 0, v3 = 0;
-      for (int j = j0; j < j1; ++j) {
-        const int n = s_cnt[s_sig[j]], g = (n + CG_P - 1) / CG_P;
-        v0 += n;
-        v1 += (g > 0) | ((g > 1) << 16);
-        v2 += (g > 2) | ((g > 3) << 16);
-        v3 += max(g - 4, 0);
-      }
-      int i0 = v0, i1 = v1, i2 = v2, i3 = v3;
+    // ---- groups: per class, prefix of the cells' group counts ---------------
+    for (int q = wid; q < 32; q += nwarps) {
+      int run = 0;
+      for (int j0 = s_coff[q]; j0 < s_coff[q + 1]; j0 += 32) {
+        const int j = j0 + lane;
+        const int h = j < s_coff[q + 1] ? s_tau[j] : 0;
+        const int g = j < s_coff[q + 1] ? (s_cnt[h] + CG_P - 1) / CG_P : 0;
+        int incl = g;
 #pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const int y0 = __shfl_up_sync(0xffffffffu, i0, off), y1 = __shfl_up_sync(0xffffffffu, i1, off);
-        const int y2 = __shfl_up_sync(0xffffffffu, i2, off), y3 = __shfl_up_sync(0xffffffffu, i3, off);
-        if (lane >= off) { i0 += y0; i1 += y1; i2 += y2; i3 += y3; }
-      }
-      if (lane == 31) { s_scan[0][wid] = i0; s_scan[1][wid] = i1; s_scan[2][wid] = i2; s_scan[3][wid] = i3; }
-      __syncthreads();
-      int e0 = i0 - v0, e1 = i1 - v1, e2 = i2 - v2, e3 = i3 - v3;
-      int t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-      for (int w = 0; w < nwarps; ++w) {
-        const int a0 = s_scan[0][w], a1 = s_scan[1][w], a2 = s_scan[2][w], a3 = s_scan[3][w];
-        if (w < wid) { e0 += a0; e1 += a1; e2 += a2; e3 += a3; }
-        t0 += a0; t1 += a1; t2 += a2; t3 += a3;
-      }
-      const int N0 = t1 & 0xffff, N1 = t1 >> 16, N2 = t2 & 0xffff, N3 = t2 >> 16;
-      const int B1 = N0, B2 = B1 + N1, B3 = B2 + N2, BO = B3 + N3;
-      NI = BO + t3;
-      unsigned* groups = reinterpret_cast<unsigned*>(sj.ux_b) + pbeg;
-      for (int j = j0; j < j1; ++j) {
-        const int h = s_sig[j], n = s_cnt[h], g = (n + CG_P - 1) / CG_P;
-        s_start[h] = e0;
-        e0 += n;
-        for (int k = 0; k < g; ++k) {
-          const int pos = k == 0 ? (e1 & 0xffff) : k == 1 ? B1 + (e1 >> 16)
-                        : k == 2 ? B2 + (e2 & 0xffff) : k == 3 ? B3 + (e2 >> 16)
-                        : BO + e3 + (k - 4);
-          groups[pos] = (unsigned)h | ((unsigned)k << 11);
+        for (int off = 1; off < 32; off <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, incl, off);
+          if (lane >= off) incl += y;
         }
-        e1 += (g > 0) | ((g > 1) << 16);
-        e2 += (g > 2) | ((g > 3) << 16);
-        e3 += max(g - 4, 0);
+        if (j < s_coff[q + 1]) s_pre[h] = run + incl - g;
+        run += __shfl_sync(0xffffffffu, incl, 31);
       }
-      if (threadIdx.x == 0) s_start[NH] = t0;
+      if (lane == 0) s_G[q] = run;
     }
     __syncthreads();
-    int* perm = sj.perm + pbeg;
-    for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
-      const int v = keyrank[ip];
-      perm[s_start[v & 2047] + (v >> 11)] = ip;
+    // level table: the first position of level l and the classes present there
+    for (int l = threadIdx.x; l < CG_LT; l += blockDim.x) {
+      int P = 0;
+      unsigned M = 0;
+      for (int c = 0; c < 32; ++c) {
+        const int n = s_G[c];
+        P += min(n, l);
+        M |= (n > l ? 1u : 0u) << c;
+      }
+      s_lvP[l] = P; s_lvM[l] = M;
+    }
+    int NI = 0;
+    for (int c = 0; c < 32; ++c) NI += s_G[c];
+    __syncthreads();
+    // position of the group of level l in class c
+    auto gpos = [&](int l, int c) {
+      if (l < CG_LT) return s_lvP[l] + __popc(s_lvM[l] & ((1u << c) - 1u));
+      int P = 0;
+      for (int c2 = 0; c2 < 32; ++c2) {
+        const int n = s_G[c2];
+        P += min(n, l) + (c2 < c && n > l ? 1 : 0);
+      }
+      return P;
+    };
+    if (pend - pbeg >= (1 << 21)) {   // beyond the slot encoding: flag, leave the tile
+      if (threadIdx.x == 0) atomicExch(&sj.counters[1], 1);
+      NI = 0;
+    } else {
+      for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
+        const int v = keyrank[ip];
+        const int h = v & 2047, r = v >> 11;
+        if (h == NH) { gs0[NI + r] = ip - pbeg; continue; }
+        const int k = r / CG_P, p = r - k * CG_P;
+        const int pos = gpos(s_pre[h] + k, cls(h));
+        const int e = (ip - pbeg) | (h << 21);
+        int* dst = p == 0 ? gs0 : p == 1 ? gs1 : p == 2 ? gs2 : gs3;
+        dst[pos] = e;
+        if (r == s_cnt[h] - 1)          // the cell's last particle closes its group
+          for (int q = p + 1; q < CG_P; ++q) (q == 1 ? gs1 : q == 2 ? gs2 : gs3)[pos] = -1;
+      }
     }
     // ---- window staged: |E|, |B| maxima and the fixed-point scale -----------
     asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -465,7 +480,6 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
     int* q_list = sj.rank_b;
     uint32_t* q_pk = sj.cell_b;
     R *q_ox = (R*)sj.ox_b, *q_oy = (R*)sj.oy_b, *q_oz = (R*)sj.oz_b;
-    const unsigned* groups = reinterpret_cast<const unsigned*>(sj.ux_b) + pbeg;
     double ke = 0.0;
     float nu2 = 0.f, nwm = 0.f;
     int nslow = 0, bad = 0;
@@ -484,11 +498,20 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
       nwm = fmaxf(nwm, fabsf(w));
     };
 
+    // the slots of a thread's next group are read one group ahead
+    int en[CG_P];
+    if ((int)threadIdx.x < NI) {
+      en[0] = gs0[threadIdx.x]; en[1] = gs1[threadIdx.x];
+      en[2] = gs2[threadIdx.x]; en[3] = gs3[threadIdx.x];
+    }
     for (int it = threadIdx.x; it < NI; it += blockDim.x) {
-      const unsigned desc = groups[it];
-      const int h = (int)(desc & 2047u), k = (int)(desc >> 11);
-      const int n = min(CG_P, s_cnt[h] - k * CG_P);
-      const int* slot = perm + s_start[h] + k * CG_P;
+      const int e[CG_P] = {en[0], en[1], en[2], en[3]};
+      if (it + (int)blockDim.x < NI) {
+        const int g = it + blockDim.x;
+        en[0] = gs0[g]; en[1] = gs1[g]; en[2] = gs2[g]; en[3] = gs3[g];
+      }
+      const int h = (int)((unsigned)e[0] >> 21);
+      const int n = 1 + (e[1] >= 0) + (e[2] >= 0) + (e[3] >= 0);
       const int hx = h % HB, hy = (h / HB) % HB, hz = h / (HB * HB);
       const int vx = hx - D, vy = hy - D, vz = hz - D;
       int ci = c0x + vx, cj = c0y + vy, ck = c0z + vz;
@@ -499,7 +522,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
       R ox[CG_P], oy[CG_P], oz[CG_P];
 #pragma unroll
       for (int p = 0; p < CG_P; ++p) {
-        ip[p] = slot[min(p, n - 1)];
+        ip[p] = pbeg + ((e[p] >= 0 ? e[p] : e[0]) & 0x1FFFFF);
         ox[p] = oxp[ip[p]]; oy[p] = oyp[ip[p]]; oz[p] = ozp[ip[p]];
       }
       // ---- gather: each window value serves the group's four particles -----
@@ -607,9 +630,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
     }
     // ---- particles outside the window: global gather and deposit ------------
     {
-      const int n_out = s_cnt[NH], o0 = s_start[NH];
+      const int n_out = s_cnt[NH];
       for (int s = threadIdx.x; s < n_out; s += blockDim.x) {
-        const int p = perm[o0 + s];
+        const int p = pbeg + gs0[NI + s];
         int ci, cj, ck;
         unpack_cell(cellp[p], ci, cj, ck);
         const R ox = oxp[p], oy = oyp[p], oz = ozp[p];

@@ -783,8 +783,8 @@ int64_t smem_bytes(int order, int prec, int acc, int tx, int ty, int tz, int dri
   i64 r = prec ? 8 : 4;
   i64 a = acc == 3 ? 8 : 4, nw = acc == 2 ? 2 : 1;
   const i64 hb = tx + 2 * drift;      // next-step occupancy histogram (fixed point)
-  if (acc == 4)                       // cell-grouped kernel: + per-cell counts and order
-    return V * 36 + hb * hb * hb * 12 + 8 + ((hb * hb * hb * 2 + 15) / 16) * 16;
+  if (acc == 4)                       // cell-grouped kernel (cg_smem_bytes)
+    return V * 36 + hb * hb * hb * 12 + 4 + ((hb * hb * hb * 2 + 15) / 16) * 16 + 256 * 8;
   return V * (6 * r + 3 * a * nw) + ((acc == 1 || acc == 2) ? hb * hb * hb * 4 : 0);
 }
 
