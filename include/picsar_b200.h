@@ -425,6 +425,10 @@ int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int3
                              const int32_t* nwork_dev, int32_t* ctr, int32_t threads,
                              int32_t ctas, int64_t smem, void* stream);
 
+/* Largest CTA size (threads) pxrb_tiled_particle_step takes with accumulator
+ * mode `acc` (host function, no GPU work). */
+int32_t pxrb_tiled_max_threads(int32_t acc);
+
 /* sizeof(pxrb_tiled_job), for bindings that mirror the struct. */
 int64_t pxrb_tiled_job_size(void);
 

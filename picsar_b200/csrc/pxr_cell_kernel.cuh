@@ -223,7 +223,6 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
   __shared__ int s_qn;
   __shared__ float s_max[5][CG_THREADS / 32];
   __shared__ double s_red[CG_THREADS / 32];
-  __shared__ int s_scan[4][CG_THREADS / 32];
   __shared__ int s_ncls[32];            // window cells per class
   __shared__ int s_coff[33];            // their start in s_tau
   __shared__ int s_G[32];               // groups per class
@@ -321,10 +320,10 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
     R *oxp = (R*)sj.ox, *oyp = (R*)sj.oy, *ozp = (R*)sj.oz;
     R *uxp = (R*)sj.ux, *uyp = (R*)sj.uy, *uzp = (R*)sj.uz;
     int* keyrank = reinterpret_cast<int*>(sj.w_b);
-    int* gs0 = sj.perm + pbeg;
-    int* gs1 = reinterpret_cast<int*>(sj.ux_b) + pbeg;
-    int* gs2 = reinterpret_cast<int*>(sj.uy_b) + pbeg;
-    int* gs3 = reinterpret_cast<int*>(sj.uz_b) + pbeg;
+    int* const gsl[4] = {sj.perm + pbeg, reinterpret_cast<int*>(sj.ux_b) + pbeg,
+                         reinterpret_cast<int*>(sj.uy_b) + pbeg,
+                         reinterpret_cast<int*>(sj.uz_b) + pbeg};
+    int* const gs0 = gsl[0];
     // ---- particles per window cell (+ the fixed-point bounds after a sort) --
     {
       int* hist = reinterpret_cast<int*>(Js) + 2 * V;   // zero; re-zeroed below
@@ -411,10 +410,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
         const int k = r / CG_P, p = r - k * CG_P;
         const int pos = gpos(s_pre[h] + k, cls(h));
         const int e = (ip - pbeg) | (h << 21);
-        int* dst = p == 0 ? gs0 : p == 1 ? gs1 : p == 2 ? gs2 : gs3;
-        dst[pos] = e;
+        gsl[p][pos] = e;
         if (r == s_cnt[h] - 1)          // the cell's last particle closes its group
-          for (int q = p + 1; q < CG_P; ++q) (q == 1 ? gs1 : q == 2 ? gs2 : gs3)[pos] = -1;
+          for (int q = p + 1; q < CG_P; ++q) gsl[q][pos] = -1;
       }
     }
     // ---- window staged: |E|, |B| maxima and the fixed-point scale -----------
@@ -501,17 +499,21 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
     // the slots of a thread's next group are read one group ahead
     int en[CG_P];
     if ((int)threadIdx.x < NI) {
-      en[0] = gs0[threadIdx.x]; en[1] = gs1[threadIdx.x];
-      en[2] = gs2[threadIdx.x]; en[3] = gs3[threadIdx.x];
+#pragma unroll
+      for (int p = 0; p < CG_P; ++p) en[p] = gsl[p][threadIdx.x];
     }
     for (int it = threadIdx.x; it < NI; it += blockDim.x) {
-      const int e[CG_P] = {en[0], en[1], en[2], en[3]};
+      int e[CG_P];
+#pragma unroll
+      for (int p = 0; p < CG_P; ++p) e[p] = en[p];
       if (it + (int)blockDim.x < NI) {
-        const int g = it + blockDim.x;
-        en[0] = gs0[g]; en[1] = gs1[g]; en[2] = gs2[g]; en[3] = gs3[g];
+#pragma unroll
+        for (int p = 0; p < CG_P; ++p) en[p] = gsl[p][it + blockDim.x];
       }
       const int h = (int)((unsigned)e[0] >> 21);
-      const int n = 1 + (e[1] >= 0) + (e[2] >= 0) + (e[3] >= 0);
+      int n = 1;
+#pragma unroll
+      for (int p = 1; p < CG_P; ++p) n += e[p] >= 0;
       const int hx = h % HB, hy = (h / HB) % HB, hz = h / (HB * HB);
       const int vx = hx - D, vy = hy - D, vz = hz - D;
       int ci = c0x + vx, cj = c0y + vy, ck = c0z + vz;

@@ -60,3 +60,7 @@ int launch_order3(int prec, int tile, int drift, int mode, const pxrb_tiled_job*
                                    threads, ctas, smem, s);
 }
 }  // namespace pxrt
+
+extern "C" int32_t pxrb_tiled_max_threads(int32_t acc) {
+  return acc == 4 ? pxrt::CG_THREADS : pxrt::MAX_THREADS;
+}

@@ -61,6 +61,7 @@ _lib.register({
     "pxrb_tiled_diagnostics": "p p p i p s",
     "pxrb_tiled_smem_bytes": "=i I I I I I I I",
     "pxrb_tiled_job_size": "=i",
+    "pxrb_tiled_max_threads": "I",
     "pxrb_tiled_diag_scratch": "=i p",
     "pxrb_tiled_diagnostics_noalloc": "p I p s",
 })
@@ -84,14 +85,13 @@ SUPPORTED_SHAPES = {(8, 1), (8, 0), (8, 2), (4, 1), (4, 0)}
 SUPPORTED_SHAPES_FP64 = {(8, 1), (8, 0), (4, 1), (4, 0)}
 # accumulator modes compiled for the FP32 engine per shape (FP64 engine: mode 3)
 SUPPORTED_ACC = {(8, 1): (0, 1, 2, 4), (8, 2): (1, 2), (4, 1): (1, 2)}
-# mode 4: the cell-grouped kernel (int32 fixed point like mode 1; FP32, shape
-# orders 1 and 3) runs CTAs of at most this many threads
-CELL_THREADS = 192
 
 
 def launch_threads(cfg, acc):
-    """CTA size of the particle kernel for a configuration and accumulator."""
-    return min(cfg.threads, CELL_THREADS) if acc == 4 else cfg.threads
+    """CTA size of the particle kernel for a configuration and accumulator:
+    mode 4 (the cell-grouped kernel) takes CTAs of at most
+    pxrb_tiled_max_threads(4) threads."""
+    return min(cfg.threads, _lib.query("pxrb_tiled_max_threads", acc))
 
 
 @dataclass

@@ -160,6 +160,9 @@ def test_langmuir_acceptance(cuda, tmp_path):
     assert np.isfinite(ex).all() and np.abs(ex).max() > 0
 
 
+# section::particle_dump precedes section::temporal: the reference reader
+# (control_file.F90:1262-1311) reads the temporal section to the end of the
+# file, so a section after it is never read.
 SMALL = """section::main
  nx = 17
  ny = 13
@@ -208,6 +211,13 @@ section::output
  dive = 1
  divb = 1
 end::output
+section::particle_dump
+ species_name = electron
+ dump_ux_min = -1e9
+ dump_uy_min = -1e9
+ dump_uz_min = -1e9
+ diag_period = 1
+end::particle_dump
 section::temporal
  frequency = 1
  kinE = 1
@@ -216,13 +226,6 @@ section::temporal
  divE-rho = 1
  rho = 1
 end::temporal
-section::particle_dump
- species_name = electron
- dump_ux_min = -1e9
- dump_uy_min = -1e9
- dump_uz_min = -1e9
- diag_period = 1
-end::particle_dump
 """
 
 
