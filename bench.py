@@ -73,9 +73,9 @@ SMEM_RATE = {"lds": 0.88, "atoms": 0.61}
 def smem_per_particle(order, acc):
     """(window loads, accumulator atomics) per particle of the fused particle
     kernel.  The cell-grouped kernel (acc 4) loads each window value once per
-    group of four particles of a cell and updates a J node once per pair."""
+    group (pair) of particles of a cell and updates a J node once per pair."""
     if acc == 4:
-        return GATHER_POINTS[order] / 4.0, DEPOSIT_UPDATES[order] / 2.0
+        return GATHER_POINTS[order] / 2.0, DEPOSIT_UPDATES[order] / 2.0
     return GATHER_POINTS[order], DEPOSIT_UPDATES[order] * (2 if acc == 2 else 1)
 
 

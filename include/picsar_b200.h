@@ -398,10 +398,11 @@ typedef struct pxrb_tiled_job {
  * 0 FP32 atomics, 1 int32 fixed point, 2 64-bit fixed point held in two
  * native int32 words (default of the FP32 engine), 3 FP64 (FP64 engine),
  * 4 int32 fixed point with the cell-grouped kernel (FP32, shape orders 1 and
- * 3, tile edge 8 with margin 1, at most 192 threads per CTA): each step sorts
- * a tile's particles by cell in shared memory and gives each thread up to
- * four particles of one cell, which share every E/B window load and sum their
- * contributions to a J node pairwise before one atomic; jobs run with it set
+ * 3, tile edge 8 with margin 1, at most pxrb_tiled_max_threads(4) threads per
+ * CTA): each step sorts a tile's particles by cell in shared memory and gives
+ * each thread a pair of particles of one cell, which share every E/B window
+ * load and sum their contributions to a J node before one atomic; jobs run
+ * with it set
  * `cell_order` so that the sort keeps cell order inside each tile.  The
  * fixed-point scales are bounded per tile from the tile's particle weights,
  * momenta, cell occupancy and fields, so no overflow is possible. */

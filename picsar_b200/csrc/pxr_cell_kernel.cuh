@@ -5,13 +5,12 @@
 // At orders 1 and 3 every particle of a cell gathers from the same E/B nodes
 // and, when it stays in its cell, deposits on the same J nodes.  The kernel
 // therefore sorts each tile's particles by window cell in shared memory at
-// the start of every step and hands each thread a group of up to four
-// particles of one cell: every E/B value the thread loads from the window
-// serves four gathers, the particles are computed as packed f32x2 pairs, and
-// a pair's Esirkepov contributions to a J node are summed in registers before
-// one shared-memory atomic.  Per particle this takes a quarter of the window
-// loads and half of the accumulator atomics of the one-particle-per-thread
-// kernel (k_tile_step), and far fewer instructions.
+// the start of every step and hands each thread a group of CG_P particles of
+// one cell (a packed f32x2 pair): every E/B value the thread loads from the
+// window serves the group's gathers, and the group's Esirkepov contributions
+// to a J node are summed in registers before one shared-memory atomic.  Per
+// particle this takes 1/CG_P of the window loads and accumulator atomics of
+// the one-particle-per-thread kernel (k_tile_step).
 #pragma once
 #include "pxr_tiled_kernel.cuh"
 
@@ -31,7 +30,7 @@ __device__ __forceinline__ f2_t f2_s(float v) { return f2_pack(v, v); }
 __device__ __forceinline__ float f2_lo(f2_t v) { return __uint_as_float((unsigned)(v & 0xffffffffull)); }
 __device__ __forceinline__ float f2_hi(f2_t v) { return __uint_as_float((unsigned)(v >> 32)); }
 
-constexpr int CG_P = 4;                 // particles per group
+constexpr int CG_P = 2;                 // particles per group (1 or 2 pairs)
 constexpr int CG_Q = CG_P / 2;          // packed pairs per group
 
 // Node shape of orders 1 and 3 at in-cell offsets o (first node at c for
@@ -154,14 +153,20 @@ __device__ __forceinline__ void cg_deposit(int* base, const f2_t (*t0)[4], const
   }
 }
 
-// CTA size: 192 threads, two CTAs per SM (168 registers per thread; a group
-// of four particles needs about that many without spilling)
-constexpr int CG_THREADS = 192;
+// CTA size: 256 threads, two CTAs per SM (128 registers per thread).  Groups
+// of two particles fit that; groups of four need 168 registers, so 12 warps
+// per SM, and measured 17.8 against 15.0 ms per step at 256^3.
+constexpr int CG_THREADS = 256;
 constexpr int CG_MINB = 2;
 
 // Entries of the per-tile level table of the group order (levels beyond it
 // are placed by a loop over the 32 classes).
 constexpr int CG_LT = 256;
+
+// Particles per thread whose window cell and rank stay in registers between
+// the count and the placement of a tile (20 x 256 threads: 5120 particles,
+// a 8^3 tile at 10 per cell); beyond that they go through global scratch.
+constexpr int CG_KR = 20;
 
 // Dynamic shared memory of the cell-grouped kernel: E/B window, int32 J
 // window, the next step's cell occupancy, per-cell counts and group
@@ -189,7 +194,7 @@ __host__ __device__ constexpr int cg_smem_bytes(int T, int D, int V) {
 //      global grid; particles outside the window take the global path.
 // Scratch, all in the tile's range of the sort buffers that are free between
 // sorts: w_b (window cell and rank per particle); perm, ux_b, uy_b, uz_b (the
-// four particle slots of each group, in group order, so a warp reads its
+// CG_P particle slots of each group, in group order, so a warp reads its
 // groups' slots with coalesced loads: tile-relative particle index | window
 // cell << 21, -1 for an empty slot; particles outside the window follow the
 // groups in perm); rank_b / cell_b / ox_b / oy_b / oz_b (the node-change
@@ -325,11 +330,12 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
                          reinterpret_cast<int*>(sj.uz_b) + pbeg};
     int* const gs0 = gsl[0];
     // ---- particles per window cell (+ the fixed-point bounds after a sort) --
+    int kr[CG_KR];
     {
       int* hist = reinterpret_cast<int*>(Js) + 2 * V;   // zero; re-zeroed below
-      for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
+      auto count = [&](int ip, uint32_t cell) {
         int ci, cj, ck;
-        unpack_cell(cellp[ip], ci, cj, ck);
+        unpack_cell(cell, ci, cj, ck);
         int vx = ci - c0x, vy = cj - c0y, vz = ck - c0z;
         if (vx > tex - 1 + D) vx -= nx; else if (vx < -D) vx += nx;
         if (vy > tey - 1 + D) vy -= ny; else if (vy < -D) vy += ny;
@@ -338,14 +344,30 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
                         vz >= -D && vz <= tez - 1 + D;
         const int key = in ? (vx + D) + HB * ((vy + D) + HB * (vz + D)) : NH;
         const int r = atomicAdd(&s_cnt[key], 1);
-        keyrank[ip] = key | (r << 11);
         if (!have) {
           const float a = uxp[ip], b = uyp[ip], c = uzp[ip];
           umax2 = fmaxf(umax2, a * a + b * b + c * c);
           wmax = fmaxf(wmax, fabsf(wp[ip]));
           if (in) atomicAdd(hist + (vx + D + L) + (vy + D + L) * SY + (vz + D + L) * SZ, 1);
         }
+        return key | (r << 11);
+      };
+      // the first CG_KR particles of each thread: cells loaded together, cell
+      // and rank kept in registers until the slots are written; the rest of a
+      // large tile through keyrank
+      uint32_t cc[CG_KR];
+#pragma unroll
+      for (int k = 0; k < CG_KR; ++k) {
+        const int ip = pbeg + threadIdx.x + k * blockDim.x;
+        cc[k] = ip < pend ? cellp[ip] : 0u;
       }
+#pragma unroll
+      for (int k = 0; k < CG_KR; ++k) {
+        const int ip = pbeg + threadIdx.x + k * blockDim.x;
+        kr[k] = ip < pend ? count(ip, cc[k]) : 0;
+      }
+      for (int ip = pbeg + threadIdx.x + CG_KR * blockDim.x; ip < pend; ip += blockDim.x)
+        keyrank[ip] = count(ip, cellp[ip]);
       __syncthreads();
       if (!have) {
         for (int r = threadIdx.x; r < V; r += blockDim.x) {
@@ -403,17 +425,23 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
       if (threadIdx.x == 0) atomicExch(&sj.counters[1], 1);
       NI = 0;
     } else {
-      for (int ip = pbeg + threadIdx.x; ip < pend; ip += blockDim.x) {
-        const int v = keyrank[ip];
+      auto place = [&](int ip, int v) {
         const int h = v & 2047, r = v >> 11;
-        if (h == NH) { gs0[NI + r] = ip - pbeg; continue; }
+        if (h == NH) { gs0[NI + r] = ip - pbeg; return; }
         const int k = r / CG_P, p = r - k * CG_P;
         const int pos = gpos(s_pre[h] + k, cls(h));
         const int e = (ip - pbeg) | (h << 21);
         gsl[p][pos] = e;
         if (r == s_cnt[h] - 1)          // the cell's last particle closes its group
           for (int q = p + 1; q < CG_P; ++q) gsl[q][pos] = -1;
+      };
+#pragma unroll
+      for (int k = 0; k < CG_KR; ++k) {
+        const int ip = pbeg + threadIdx.x + k * blockDim.x;
+        if (ip < pend) place(ip, kr[k]);
       }
+      for (int ip = pbeg + threadIdx.x + CG_KR * blockDim.x; ip < pend; ip += blockDim.x)
+        place(ip, keyrank[ip]);
     }
     // ---- window staged: |E|, |B| maxima and the fixed-point scale -----------
     asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -521,13 +549,14 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
       cj = cj < 0 ? cj + ny : (cj >= ny ? cj - ny : cj);
       ck = ck < 0 ? ck + nz : (ck >= nz ? ck - nz : ck);
       int ip[CG_P];
-      R ox[CG_P], oy[CG_P], oz[CG_P];
+      R ox[CG_P], oy[CG_P], oz[CG_P], u0[CG_P], u1[CG_P], u2[CG_P], wg[CG_P];
 #pragma unroll
       for (int p = 0; p < CG_P; ++p) {
         ip[p] = pbeg + ((e[p] >= 0 ? e[p] : e[0]) & 0x1FFFFF);
         ox[p] = oxp[ip[p]]; oy[p] = oyp[ip[p]]; oz[p] = ozp[ip[p]];
+        u0[p] = uxp[ip[p]]; u1[p] = uyp[ip[p]]; u2[p] = uzp[ip[p]]; wg[p] = wp[ip[p]];
       }
-      // ---- gather: each window value serves the group's four particles -----
+      // ---- gather: each window value serves the group's particles -----------
       R eb[6][CG_P];
       {
         f2_t nX[CG_Q][4], nY[CG_Q][4], nZ[CG_Q][4], sX[CG_Q][4], sY[CG_Q][4], sZ[CG_Q][4];
@@ -559,8 +588,8 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
 #pragma unroll
       for (int p = 0; p < CG_P; ++p) {
         const bool valid = p < n;
-        R ux = uxp[ip[p]], uy = uyp[ip[p]], uz = uzp[ip[p]];
-        const R wgt = wp[ip[p]];
+        R ux = u0[p], uy = u1[p], uz = u2[p];
+        const R wgt = wg[p];
         R gi;
         if (vay) {
           gi = inv_sqrt<R>((R)1 + (ux * ux + uy * uy + uz * uz) * clghtisq);

@@ -2,14 +2,14 @@
 int32 fixed-point current, shape orders 1 and 3) against the CPU oracle,
 through the C ABI.
 
-The kernel sorts each tile's particles by cell every step and computes up
-to four particles of a cell per thread; its bars are those of the int32
+The kernel sorts each tile's particles by cell every step and computes a
+pair of particles of a cell per thread; its bars are those of the int32
 fixed-point accumulator (mode 1): relative L2 <= 2e-4 for E, B and J (the
 J quantisation of one int32 word) and 1e-6 for momenta after one step, and
 a Gauss-law residual drift below 1e-5 over 20 steps.  Cases: thermal
 plasma (most cells with one or two groups), hot plasma stepped without
 re-sorting (cell changes, particles outside the window), dense cells
-(groups past the fourth round), partial tiles and an empty job.
+(hundreds of groups per cell), partial tiles and an empty job.
 """
 import numpy as np
 import pytest
