@@ -559,13 +559,16 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
       // ---- gather: each window value serves the group's particles -----------
       R eb[6][CG_P];
       {
-        f2_t nX[CG_Q][4], nY[CG_Q][4], nZ[CG_Q][4], sX[CG_Q][4], sY[CG_Q][4], sZ[CG_Q][4];
+        // node shapes for all six components; the staggered ones computed where
+        // needed, in a component order that keeps at most two of them live
+        f2_t ax[CG_Q], ay[CG_Q], az[CG_Q];
+        f2_t nX[CG_Q][4], nY[CG_Q][4], nZ[CG_Q][4], sA[CG_Q][4], sB[CG_Q][4];
 #pragma unroll
         for (int q = 0; q < CG_Q; ++q) {
-          const f2_t ax = f2_pack(ox[2 * q], ox[2 * q + 1]), ay = f2_pack(oy[2 * q], oy[2 * q + 1]),
-                     az = f2_pack(oz[2 * q], oz[2 * q + 1]);
-          node_pair<ORDER>(ax, nX[q]); node_pair<ORDER>(ay, nY[q]); node_pair<ORDER>(az, nZ[q]);
-          stag_pair<ORDER>(ax, sX[q]); stag_pair<ORDER>(ay, sY[q]); stag_pair<ORDER>(az, sZ[q]);
+          ax[q] = f2_pack(ox[2 * q], ox[2 * q + 1]); ay[q] = f2_pack(oy[2 * q], oy[2 * q + 1]);
+          az[q] = f2_pack(oz[2 * q], oz[2 * q + 1]);
+          node_pair<ORDER>(ax[q], nX[q]); node_pair<ORDER>(ay[q], nY[q]);
+          node_pair<ORDER>(az[q], nZ[q]);
         }
         // gather and deposit stencils of a cell both start at its window address
         const float* F = Fs + hx + hy * SY + hz * SZ;
@@ -575,12 +578,19 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
   _Pragma("unroll") for (int q = 0; q < CG_Q; ++q) {                                          \
     eb[c_][2 * q] = f2_lo(o2[q]); eb[c_][2 * q + 1] = f2_hi(o2[q]);                           \
   }
-        PXRB_CG_COMP(0, S, N, N, sX, nY, nZ)
-        PXRB_CG_COMP(1, N, S, N, nX, sY, nZ)
-        PXRB_CG_COMP(2, N, N, S, nX, nY, sZ)
-        PXRB_CG_COMP(3, N, S, S, nX, sY, sZ)
-        PXRB_CG_COMP(4, S, N, S, sX, nY, sZ)
-        PXRB_CG_COMP(5, S, S, N, sX, sY, nZ)
+#define PXRB_CG_STAG(dst_, o_) \
+  _Pragma("unroll") for (int q = 0; q < CG_Q; ++q) stag_pair<ORDER>(o_[q], dst_[q]);
+        PXRB_CG_STAG(sA, ax)                         // sA = x
+        PXRB_CG_COMP(0, S, N, N, sA, nY, nZ)         // Ex
+        PXRB_CG_STAG(sB, az)                         // sB = z
+        PXRB_CG_COMP(4, S, N, S, sA, nY, sB)         // By
+        PXRB_CG_COMP(2, N, N, S, nX, nY, sB)         // Ez
+        PXRB_CG_STAG(sA, ay)                         // sA = y
+        PXRB_CG_COMP(3, N, S, S, nX, sA, sB)         // Bx
+        PXRB_CG_COMP(1, N, S, N, nX, sA, nZ)         // Ey
+        PXRB_CG_STAG(sB, ax)                         // sB = x
+        PXRB_CG_COMP(5, S, S, N, sB, sA, nZ)         // Bz
+#undef PXRB_CG_STAG
 #undef PXRB_CG_COMP
       }
       // ---- push, position, store; deposit factors ------------------------------
