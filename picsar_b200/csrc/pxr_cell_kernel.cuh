@@ -397,8 +397,11 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
       if (lane == 0) s_G[q] = run;
     }
     __syncthreads();
-    // level table: the first position of level l and the classes present there
-    for (int l = threadIdx.x; l < CG_LT; l += blockDim.x) {
+    // level table: the first position of level l and the classes present
+    // there, for the levels that occur (below the largest class)
+    int NI = 0, Gmax = 0;
+    for (int c = 0; c < 32; ++c) { NI += s_G[c]; Gmax = max(Gmax, s_G[c]); }
+    for (int l = threadIdx.x; l < min(Gmax, CG_LT); l += blockDim.x) {
       int P = 0;
       unsigned M = 0;
       for (int c = 0; c < 32; ++c) {
@@ -408,8 +411,6 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MINB)
       }
       s_lvP[l] = P; s_lvM[l] = M;
     }
-    int NI = 0;
-    for (int c = 0; c < 32; ++c) NI += s_G[c];
     __syncthreads();
     // position of the group of level l in class c
     auto gpos = [&](int l, int c) {
