@@ -87,6 +87,28 @@ def smem_floor_ms(order, acc, particles, sms, clock_mhz):
     return particles / 32.0 * clk_per_warp / sms / (clock_mhz * 1e6) * 1e3
 GRID_BYTES_PER_CELL = {0: (24 + 48), 1: (48 + 48)}        # E,B read + J FP64 read-modify-write
 
+def particle_flops(order):
+    """Algorithmic floating-point operations of one particle-step of the
+    particle kernel at a shape order (mul / add / sub / sqrt / divide count
+    one, an FMA two), counted from the loops of the oracle's restatement of
+    the reference with the tensor-product gather factored (x, then y, then z):
+      gather shapes  node and staggered shape per axis (orders 1/2/3: 1/10/24);
+      gather         per component a*b*c + b*c + c FMAs over its stencil
+                     (a, b, c = node or staggered extents of the component);
+      push           Boris (68) + set_gamma (8);
+      position       5 per axis;
+      deposit shapes new and old node shapes per axis (1/8/15 each);
+      deposit        per component of the no-node-change Esirkepov box of
+                     N = order+1 nodes per axis: prefix 2N-3, ds N, A and B
+                     5N, weights 4N^2, node updates 2 N^2 (N-1);
+      energy         11."""
+    n, s = order + 1, order
+    shape = {1: (1, 0), 2: (8, 2), 3: (15, 9)}[order]
+    comps = [(s, n, n), (n, s, n), (n, n, s), (n, s, s), (s, n, s), (s, s, n)]
+    gather = sum(2 * (a * b * c + b * c + c) for a, b, c in comps)
+    deposit = 3 * ((2 * n - 3) + n + 5 * n + 4 * n * n + 2 * n * n * (n - 1))
+    return (3 * sum(shape) + gather + 76 + 15 + 6 * shape[0] + deposit + 11)
+
 
 def _initial_state(wl, seed, n=None, device="cuda"):
     """Seeded synthetic initial plasma of a workload (optionally on a
@@ -483,11 +505,13 @@ def run_ours(args, emit=True):
                        "tile_occupancy": occupancy},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": f"k_tiled_step<{'float' if prec == 0 else 'double'},"
-                                   f"{wl['order']}>",
+                         "kernel": (f"k_cell_step<{wl['order']}>" if cfg.acc == 4 else
+                                    f"k_tile_step<{'float' if prec == 0 else 'double'},"
+                                    f"{wl['order']}>"),
                          "kernel_ms": kern_ms, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},
             "smem_roofline": _smem_roofline(wl, prec, cfg, N, kern_ms, clk),
+            "compute_roofline": _compute_roofline(wl, prec, N, kern_ms),
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
@@ -508,6 +532,22 @@ def run_ours(args, emit=True):
         import torch.distributed as dist
         dist.destroy_process_group()
     return line if rank == 0 else None
+
+
+def _compute_roofline(wl, prec, N, kern_ms):
+    """The particle kernel against the measured FMA throughput of this GPU's
+    CUDA cores (the tensor cores have no part in the particle step): FP32
+    engine against the faster of scalar FP32 and packed f32x2 FMA, FP64
+    engine against FP64 FMA (picsar_b200.peaks, about 3 s of probes; packed
+    f32x2 FMAs measured no faster than scalar ones on B200)."""
+    from picsar_b200 import peaks
+    p = peaks.fma_peaks(iters=4096, repeats=2)
+    peak = max(p["fp32"], p["fp32x2"]) if prec == 0 else p["fp64"]
+    fl = particle_flops(wl["order"])
+    achieved = fl * N / (kern_ms * 1e-3) / 1e12
+    return {"bound": "fp32" if prec == 0 else "fp64", "flop_per_particle_step": fl,
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peaks_measured": p, "peak_kind": "measured (pxrb_fma_probe)"}
 
 
 def _smem_roofline(wl, prec, cfg, N, kern_ms, clk):

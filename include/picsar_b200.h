@@ -426,6 +426,18 @@ int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int3
                              const int32_t* nwork_dev, int32_t* ctr, int32_t threads,
                              int32_t ctas, int64_t smem, void* stream);
 
+/* Arithmetic-throughput probe (no counterpart in the reference; it measures
+ * the compute ceiling the particle kernels are compared with): `blocks` x
+ * `threads` threads each run 8 independent chains a <- a*b + c for `iters`
+ * rounds, kind 0 in FP32, 1 in packed f32x2 (two FP32 FMAs per instruction),
+ * 2 in FP64, and write the sum of their chains to sink (DEVICE float[blocks *
+ * threads]).  With b = 1 every chain ends at its start value + iters * c.
+ * pxrb_fma_probe_flops gives the launch's floating-point operations (an FMA
+ * counts two), or -1 for bad arguments (host function). */
+int pxrb_fma_probe(int32_t kind, int32_t blocks, int32_t threads, int32_t iters, float b,
+                   float c, float* sink, void* stream);
+int64_t pxrb_fma_probe_flops(int32_t kind, int32_t blocks, int32_t threads, int32_t iters);
+
 /* Largest CTA size (threads) pxrb_tiled_particle_step takes with accumulator
  * mode `acc` (host function, no GPU work). */
 int32_t pxrb_tiled_max_threads(int32_t acc);

@@ -63,7 +63,7 @@ for _o in (1, 2, 3):
     _SIGS[f"pxrb_field_gathering_plus_particle_pusher_{_o}_{_o}_{_o}"] = (
         "i" + " p" * 13 + " d" * 7 + " i" * 6 + " p" * 6 + " d d i i d i d s")
 
-_CT = {"i": i64, "d": f64, "p": P, "s": P, "I": I32}
+_CT = {"i": i64, "d": f64, "p": P, "s": P, "I": I32, "f": C.c_float}
 
 _lib = None
 

@@ -14,7 +14,7 @@ def _declared():
             continue
         src = open(os.path.join(ROOT, "include", fn)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        names |= set(re.findall(r"\b(?:int|int64_t)\s+(pxrb_\w+)\s*\(", src))
+        names |= set(re.findall(r"\b(?:int|int32_t|int64_t)\s+(pxrb_\w+)\s*\(", src))
         for o in re.findall(r"PXRB_FGP_DECL\((\d)\)\s*$", src, flags=re.M):
             names.add(f"pxrb_field_gathering_plus_particle_pusher_{o}_{o}_{o}")
     names.discard("pxrb_field_gathering_plus_particle_pusher_")
@@ -33,6 +33,7 @@ def test_library_exports_all_declared_symbols():
 def test_python_signatures_cover_header():
     from picsar_b200 import _lib
     import picsar_b200.ensemble  # noqa: F401  (these modules register their signatures)
+    import picsar_b200.peaks  # noqa: F401
     import picsar_b200.picsar  # noqa: F401
     import picsar_b200.psatd  # noqa: F401
     import picsar_b200.tiled  # noqa: F401
