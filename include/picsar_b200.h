@@ -401,8 +401,9 @@ typedef struct pxrb_tiled_job {
  * 3, tile edge 8 with margin 1, at most pxrb_tiled_max_threads(4) threads per
  * CTA): each step sorts a tile's particles by cell in shared memory and gives
  * each thread a pair of particles of one cell, which share every E/B window
- * load and sum their contributions to a J node before one atomic; jobs run
- * with it set
+ * load and sum their contributions to a J node before one atomic (tiles of
+ * fewer than 2^21 particles: a larger tile sets the error flag and is left
+ * unprocessed); jobs run with it set
  * `cell_order` so that the sort keeps cell order inside each tile.  The
  * fixed-point scales are bounded per tile from the tile's particle weights,
  * momenta, cell occupancy and fields, so no overflow is possible. */
