@@ -66,8 +66,8 @@ __device__ __forceinline__ void stag_pair(f2_t o, f2_t* s) {
 
 // One field component at the group's CG_P particles: window points
 // base[t + b*SY + c*SZ], weights sa[q][t] * sb[q][b] * sc[q][c] of pair q.
-// Each loaded value is splatted once and serves both pairs; per particle the
-// sums run as gwin's (x, then y, then z).
+// Each loaded value is splatted once and serves the group's pairs; per
+// particle the sums run as gwin's (x, then y, then z).
 template <int NA, int NB, int NC, int SY, int SZ>
 __device__ __forceinline__ void cg_comp(const float* base, const f2_t (*sa)[4],
                                         const f2_t (*sb)[4], const f2_t (*sc)[4],
@@ -182,7 +182,7 @@ __host__ __device__ constexpr int cg_smem_bytes(int T, int D, int V) {
 //   1. the E/B window is staged with cp.async while the tile's particles are
 //      counted per window cell (one shared atomic each; particles outside
 //      the window go to one more bucket), and the counts are scanned;
-//   2. each window cell of n particles makes ceil(n/4) groups; a group's
+//   2. each window cell of n particles makes ceil(n/CG_P) groups; a group's
 //      bank class is its cell's (the bank of the cell's window address, where
 //      its gather loads and deposit atomics start); the groups are numbered
 //      within their class (level) and laid out by (level, class), so 32
