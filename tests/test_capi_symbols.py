@@ -40,3 +40,23 @@ def test_python_signatures_cover_header():
     declared = _declared()
     missing = sorted(declared - set(_lib.exported_symbols()))
     assert not missing, missing
+
+
+def test_probe_flop_count_host():
+    """pxrb_fma_probe_flops is a host function: the FLOPs of a probe launch
+    (8 FMA chains per thread, an FMA counting two, packed f32x2 twice)."""
+    from picsar_b200 import _lib
+    import picsar_b200.peaks  # noqa: F401
+    assert _lib.query("pxrb_fma_probe_flops", 0, 2, 64, 10) == 2 * 64 * 10 * 8 * 2
+    assert _lib.query("pxrb_fma_probe_flops", 1, 2, 64, 10) == 2 * 64 * 10 * 8 * 2 * 2
+    assert _lib.query("pxrb_fma_probe_flops", 2, 3, 32, 7) == 3 * 32 * 7 * 8 * 2
+    assert _lib.query("pxrb_fma_probe_flops", 3, 1, 32, 1) == -1
+    assert _lib.query("pxrb_fma_probe_flops", 0, 0, 32, 1) == -1
+
+
+def test_max_threads_host():
+    """The particle kernel's largest CTA per accumulator mode (host function)."""
+    from picsar_b200 import _lib
+    import picsar_b200.tiled  # noqa: F401
+    assert _lib.query("pxrb_tiled_max_threads", 1) == 256
+    assert _lib.query("pxrb_tiled_max_threads", 4) == 256
