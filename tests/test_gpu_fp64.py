@@ -1,7 +1,6 @@
 """Parity of the plain FP64 CUDA path against the CPU oracle.
 
-Bar: relative L2 <= 1e-12 on the same seeded inputs (FP64 mode of the
-north-star contract).  Each test calls the C ABI through the Forthon-named
+Bar: relative L2 <= 1e-12 on the same seeded inputs (the FP64 bar).  Each test calls the C ABI through the Forthon-named
 wrappers in picsar_b200.picsar.
 """
 import numpy as np
