@@ -62,7 +62,7 @@ BYTES_PER_PARTICLE = {0: (32 + 28), 1: (60 + 52)}        # particle kernel, per 
 # Shared-memory work of the fused particle kernel per particle (FP32 engine):
 # energy-conserving gather points (E: 3*S*N*N, B: 3*N*S*S; N = order+1,
 # S = order) and fast-path Esirkepov accumulator updates (3*(N-1)*N*N, per
-# fixed-point word).  Conflict-free shared-memory rates of this pool's B200,
+# fixed-point word).  Conflict-free shared-memory rates of the B200,
 # warp-instructions per clock per SM, measured with a 32-bit load / 32-bit
 # atomic-add probe at 8-64 resident warps: LDS.32 0.88, ATOMS.32 0.61.
 GATHER_POINTS = {1: 18, 2: 90, 3: 252}
