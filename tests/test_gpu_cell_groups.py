@@ -122,6 +122,35 @@ def test_cell_groups_dense_cells(cuda, order):
 
 
 @pytest.mark.parametrize("order", [1, 3])
+def test_cell_groups_crowded_tile(cuda, order):
+    """7000 particles in one 8^3 tile (14 per cell): more than the 20 per
+    thread whose cell and rank the kernel keeps in registers, so the rest go
+    through the global scratch between count and placement.  Two steps
+    against the oracle, to the int32 accumulator's resolution: mode 4 as
+    close as mode 1."""
+    n, g = (16, 16, 16), 3
+    rng = np.random.default_rng(2300 + order)
+    m = 7000
+    st = {c: 8.0 * rng.random(m) for c in ("x", "y", "z")}
+    for c in ("ux", "uy", "uz"):
+        st[c] = 0.05 * rng.standard_normal(m)
+    st["w"] = np.full(m, 1.0 / 14.0)
+    fields = random_fields(n, g, seed=2350 + order, amp=0.02)
+    errs = {}
+    for acc in (1, 4):
+        o, t = _pair(n, order, 0, "fp32", st, TiledConfig(tile=(8, 8, 8), drift=1, acc=acc),
+                     fields)
+        o.step(2)
+        t.step(2, keep_j=True)
+        errs[acc] = _errors(o, t, g)
+        assert t.error_flag() == 0
+    for k, e4 in errs[4].items():
+        e1 = errs[1][k]
+        assert e4 <= (1e-5 if k.startswith("p_") else 1e-3), (k, e4, e1)
+        assert e4 <= 1.5 * e1 + (1e-7 if k.startswith("p_") else 2e-5), (k, e4, e1)
+
+
+@pytest.mark.parametrize("order", [1, 3])
 def test_cell_groups_partial_tiles(cuda, order):
     """Grid extents that are not multiples of the tile edge (partial tiles,
     periodic wrap inside a window), particles on cell faces and just below
