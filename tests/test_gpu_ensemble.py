@@ -88,6 +88,22 @@ def test_ensemble_fp32_matches_jobs_alone(cuda):
         _cmp(sim, _alone(spec, "fp32", cfgs[spec.order]), 1e-5)
 
 
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_ensemble_cell_groups_match_jobs_alone(cuda, use_graph):
+    """Orders 1 and 3 on the cell-grouped kernel (accumulator mode 4) in a
+    batch: the batched sort keeps each job's cell order, the batched step
+    launches the kernel's CTA size and skips the bank re-layout, and every
+    job ends where it does alone (to the order of the FP64 flush atomics)."""
+    cell = TiledConfig(tile=(8, 8, 8), drift=1, acc=4, sort_interval=2, relayout_interval=1)
+    cfgs = {1: cell, 2: TiledConfig(tile=(8, 8, 8), sort_interval=3), 3: cell}
+    ens = Ensemble(SPECS, precision="fp32", configs=cfgs, track_ids=True, use_graph=use_graph)
+    ens.step(6)
+    torch.cuda.synchronize()
+    assert all(f == 0 for f in ens.error_flags())
+    for spec, sim in ens.sims():
+        _cmp(sim, _alone(spec, "fp32", cfgs[spec.order]), 1e-5)
+
+
 def test_batched_sort_layout_matches_single_job_sort(cuda):
     """After one batched sort every job has the same tile offsets and the
     same set of particles per tile as after its own single-job sort."""
