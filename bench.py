@@ -925,8 +925,9 @@ def run_tiled_fp64(wl, args, ws, rank, cfg):
             "roofline": {"bound": "hbm", "achieved": alg / (kern * 1e-3) / 1e9, "peak": peak,
                          "unit": "GB/s", "frac": alg / (kern * 1e-3) / 1e9 / peak,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg},
+            "threads": c64.fp64_threads,
             "what": "tiled engine in FP64 (within 1e-12 of the oracle), same tiles and sort "
-                    "interval, no re-layout (the FP64 kernel makes one pass)"}
+                    "interval, no re-layout (the FP64 kernel makes one pass), one CTA per SM"}
 
 
 def _plain_fp64_jobs(specs, steps=2):

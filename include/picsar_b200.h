@@ -419,7 +419,8 @@ typedef struct pxrb_tiled_job {
  * path.  jobs_dev: DEVICE descriptors (all of this `order` and `prec`);
  * work: DEVICE int32 pairs (job, tile), nwork of them (nwork_dev, if not
  * NULL, a DEVICE count <= nwork read at run time); ctr: DEVICE int32 reset by
- * the call; threads: CTA size, multiple of 32, <= 256; smem: dynamic shared
+ * the call; threads: CTA size, multiple of 32, <= pxrb_tiled_max_threads(acc)
+ * (256; 512 for the FP64 engine, which runs one CTA per SM); smem: dynamic shared
  * memory bytes, >= pxrb_tiled_smem_bytes() of the largest tile window. */
 int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int32_t prec,
                              int32_t tile, int32_t drift, int32_t acc, const int32_t* work,

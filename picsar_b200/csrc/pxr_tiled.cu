@@ -812,7 +812,9 @@ int pxrb_tiled_particle_step(const pxrb_tiled_job* jobs_dev, int32_t order, int3
                              int32_t ctas, int64_t smem, void* stream) {
   if (!jobs_dev || !work || !ctr || nwork < 0 || smem < 0) return PXRB_EINVAL;
   if (nwork == 0) return PXRB_OK;
-  if (threads < 32 || threads > MAX_THREADS || threads % 32) return PXRB_EINVAL;
+  if (threads < 32 || threads % 32 ||
+      threads > (prec == 1 && acc != 4 ? MAX_THREADS_FP64 : MAX_THREADS))
+    return PXRB_EINVAL;
   if (order < 1 || order > 3 || prec < 0 || prec > 1) return PXRB_EUNSUPPORTED;
   if (ctas < 1) ctas = 1;
   cudaStream_t s = (cudaStream_t)stream;

@@ -559,7 +559,9 @@ __device__ __forceinline__ void f2_splat(const float* s, f2_t* s2) {
   for (int i = 0; i < N; ++i) s2[i] = f2_pack(s[i], s[i]);
 }
 
-constexpr int MAX_THREADS = 256;
+constexpr int MAX_THREADS = 256;        // FP32 engine: two CTAs per SM
+constexpr int MAX_THREADS_FP64 = 512;   // FP64 engine: one CTA per SM
+constexpr int MAX_WARPS = MAX_THREADS_FP64 / 32;
 
 // Window particles whose Esirkepov node changes along some axis are queued
 // and deposited after the tile's main loop by full warps, so the common
@@ -582,8 +584,13 @@ __device__ __forceinline__ float warp_max(float v) {
 // immediate.  Windows of partial tiles extend into the padded guard region of
 // the field arrays (never written, zero) which no particle reaches.
 // ---------------------------------------------------------------------------
+// FP32 windows fit two CTAs of 256 threads per SM (128 registers per
+// thread); the FP64 engine's windows take one CTA per SM, of up to 512
+// threads (128 registers): its FP64 shared atomics want the warps (256 /
+// 384 / 512 / 640 threads measured 76.6 / 63.5 / 58.0 / 58.8 ms at 256^3).
 template <typename R, int ORDER, int T, int D, int MODE>
-__global__ void __launch_bounds__(MAX_THREADS, 2)
+__global__ void __launch_bounds__(sizeof(R) == 8 ? MAX_THREADS_FP64 : MAX_THREADS,
+                                  sizeof(R) == 8 ? 1 : 2)
     k_tile_step(const Job* __restrict__ jobs, const int2* __restrict__ work, int nwork,
                 const int* __restrict__ nwork_dev, int* ctr) {
   constexpr int L = Reach<ORDER>::L, H = Reach<ORDER>::H;
@@ -604,8 +611,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 2)
   constexpr bool SELECT = sizeof(R) == 4;
   __shared__ int s_dn;                             // deferred particles of the tile
   __shared__ int s_dcnt[32];                       // ... per bank class
-  __shared__ float s_max[5][MAX_THREADS / 32];
-  __shared__ double s_red[MAX_THREADS / 32];
+  __shared__ float s_max[5][MAX_WARPS];
+  __shared__ double s_red[MAX_WARPS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 
   if (nwork_dev) nwork = min(nwork, *nwork_dev);

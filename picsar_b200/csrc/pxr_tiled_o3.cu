@@ -62,5 +62,5 @@ int launch_order3(int prec, int tile, int drift, int mode, const pxrb_tiled_job*
 }  // namespace pxrt
 
 extern "C" int32_t pxrb_tiled_max_threads(int32_t acc) {
-  return acc == 4 ? pxrt::CG_THREADS : pxrt::MAX_THREADS;
+  return acc == 4 ? pxrt::CG_THREADS : acc == 3 ? pxrt::MAX_THREADS_FP64 : pxrt::MAX_THREADS;
 }

@@ -89,9 +89,10 @@ SUPPORTED_ACC = {(8, 1): (0, 1, 2, 4), (8, 2): (1, 2), (4, 1): (1, 2)}
 
 def launch_threads(cfg, acc):
     """CTA size of the particle kernel for a configuration and accumulator:
-    mode 4 (the cell-grouped kernel) takes CTAs of at most
-    pxrb_tiled_max_threads(4) threads."""
-    return min(cfg.threads, _lib.query("pxrb_tiled_max_threads", acc))
+    `threads` for the FP32 engine, `fp64_threads` for the FP64 one (mode 3),
+    each at most pxrb_tiled_max_threads(acc)."""
+    want = cfg.fp64_threads if acc == 3 else cfg.threads
+    return min(want, _lib.query("pxrb_tiled_max_threads", acc))
 
 
 @dataclass
@@ -105,6 +106,7 @@ class TiledConfig:
     relayout_interval: int = 4  # bank-order re-layout of the tiles between sorts (0: none)
     acc: int = 2                # FP32 engine current accumulator (see picsar_b200.h)
     select_lanes: bool = True   # FP32 engine: distinct bank classes per warp, second pass
+    fp64_threads: int = 512     # FP64 engine's CTA size (one CTA per SM; `threads` is FP32's)
 
 
 def h2d_bytes(buf):
