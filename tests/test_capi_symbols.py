@@ -60,3 +60,4 @@ def test_max_threads_host():
     import picsar_b200.tiled  # noqa: F401
     assert _lib.query("pxrb_tiled_max_threads", 1) == 256
     assert _lib.query("pxrb_tiled_max_threads", 4) == 256
+    assert _lib.query("pxrb_tiled_max_threads", 3) == 512
