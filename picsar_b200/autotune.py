@@ -6,7 +6,8 @@ For a (shape order, precision, particles per cell, thermal spread, beam
 drift) class of jobs, a proxy simulation large enough to occupy every SM (at least two tiles
 per resident CTA) is stepped under each candidate and timed with CUDA events
 on the launching stream.  Stage 1 times every compiled (tile edge, margin)
-pair at both thread counts over 20 steps with a sort every 5 steps; stage 2
+pair at both thread counts (FP64: 256 and 512 threads, one CTA per SM)
+over 20 steps with a sort every 5 steps; stage 2
 times the two best at each pair of sort interval and bank re-layout interval
 over 40 steps (the slow path for particles that drifted out of their tile
 window, the bank conflicts of particles that changed cell, and the sorts
@@ -23,7 +24,7 @@ from __future__ import annotations
 import json
 import math
 import os
-from dataclasses import asdict, dataclass, field
+from dataclasses import asdict, dataclass, field, replace
 
 import torch
 
@@ -32,6 +33,7 @@ from ._lib import PicsarB200Error
 from .tiled import SUPPORTED_ACC, SUPPORTED_SHAPES, TiledConfig, TiledSim
 
 THREADS = (128, 256)
+THREADS_FP64 = (256, 512)     # the FP64 engine runs one CTA per SM
 SORT_INTERVALS = (5, 10, 20, 40)
 RELAYOUT_INTERVALS = (0, 2, 4)
 
@@ -63,7 +65,7 @@ def _key(order, precision, ppc, sigma, pusher, u_drift=0.0, device_name=None, ac
     sb = round(math.log10(max(sigma, 1e-6)) * 2) / 2
     db = f"|d{round(u_drift, 2)}" if u_drift else ""
     ab = f"|a{acc}" if precision == "fp32" else ""
-    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}{db}|p{pusher}{ab}|v6"
+    return f"{name}|o{order}|{precision}|ppc{ppc}|s{sb}{db}|p{pusher}{ab}|v7"
 
 
 def acc_for(edge, drift, acc, order=3):
@@ -139,12 +141,14 @@ def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
         shapes = sorted(SUPPORTED_SHAPES)
     table = []
     ranked = []
+    fp64 = precision == "fp64"
     for edge, drift in shapes:
-        for th in threads:
+        for th in (THREADS_FP64 if fp64 and threads == THREADS else threads):
             # a short sort interval, so that shapes are ranked by the kernel
             # rather than by the slow path of particles that left their window
-            cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, threads=th, sort_interval=5,
-                              relayout_interval=0, acc=acc_for(edge, drift, acc, order))
+            cfg = TiledConfig(tile=(edge, edge, edge), drift=drift, sort_interval=5,
+                              relayout_interval=0, acc=acc_for(edge, drift, acc, order),
+                              **({"fp64_threads": th} if fp64 else {"threads": th}))
             try:
                 r = _time(cfg, order, precision, st, n, 20, pusher)
             except (ValueError, RuntimeError, PicsarB200Error) as e:   # not compiled here
@@ -161,10 +165,10 @@ def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
             for R in relayout_intervals:
                 if R >= K:
                     continue
-                cfg = TiledConfig(tile=cfg0.tile, drift=cfg0.drift, threads=cfg0.threads,
-                                  sort_interval=K, relayout_interval=R, acc=cfg0.acc)
+                cfg = replace(cfg0, sort_interval=K, relayout_interval=R)
                 r = _time(cfg, order, precision, st, n, 40, pusher)
-                table.append((cfg0.tile[0], cfg0.drift, cfg0.threads, K, R, r))
+                th = cfg0.fp64_threads if fp64 else cfg0.threads
+                table.append((cfg0.tile[0], cfg0.drift, th, K, R, r))
                 if best is None or r > best[1]:
                     best = (cfg, r)
     # stage 3 (FP32): the winner in one pass, without the bank-class lane
@@ -172,9 +176,7 @@ def tune(order, precision="fp32", ppc=8, sigma=0.01, pusher=0, use_cache=True,
     # change cell every step)
     if precision == "fp32":
         c1 = best[0]
-        cfg = TiledConfig(tile=c1.tile, drift=c1.drift, threads=c1.threads,
-                          sort_interval=c1.sort_interval, relayout_interval=c1.relayout_interval,
-                          acc=c1.acc, select_lanes=False)
+        cfg = replace(c1, select_lanes=False)
         r = _time(cfg, order, precision, st, n, 40, pusher)
         table.append((c1.tile[0], c1.drift, c1.threads, c1.sort_interval, c1.relayout_interval,
                       r, "one pass"))
